@@ -1,0 +1,325 @@
+// Breadth-first search, level output.
+//
+// Reference semantics: lonestar/analytics/cpu/bfs/bfs.cpp:244-293 (SyncTile:
+// level-synchronous, `if level[dst]==INF {level[dst]=nextLevel; push}`), with
+// the push/pull switch of bfsDirectionOpt.cpp:204-342 (alpha=15, beta=18).
+// Levels are unique, so the result is bit-identical to the CPU app whatever
+// the schedule.
+//
+// B200 design: ONE cooperative persistent launch runs every level.  A level is
+// either
+//   push (top-down): warps grab 32 frontier vertices at a time from the light
+//        queue and expand them cooperatively (degree prefix sum + shuffle
+//        owner search, coalesced column reads); vertices above heavy_degree
+//        were queued as edge tiles of tile_edges arcs, which any warp can take;
+//        discovery = check-before-atomicOr on a visited bitmap (2 MB for 16M
+//        vertices, L2 resident), warp-aggregated queue appends;
+//   pull (bottom-up): every unvisited vertex scans its in-edges until it finds
+//        a parent in the frontier bitmap.
+// Every discovered vertex is written to both the next queue and the next
+// frontier bitmap, so either direction can follow without a conversion pass.
+// Levels are separated by a bounded software grid barrier.
+
+#include "device_common.cuh"
+#include "device_graph.cuh"
+#include "frontier.cuh"
+
+namespace gb {
+
+namespace {
+
+struct BfsCtl {
+  GridBar bar;
+  int err;
+  uint32_t pad0;
+  FrontierCounters fc[3];
+  unsigned long long scanned;
+  uint32_t levels;
+  uint32_t pull_levels;
+  unsigned long long reached;
+  unsigned long long reached_deg;
+};
+
+struct BfsArgs {
+  const uint64_t* __restrict__ offs;
+  const uint32_t* __restrict__ col;
+  const uint64_t* __restrict__ in_offs;  // nullptr: push only
+  const uint32_t* __restrict__ in_col;
+  uint32_t n;
+  uint64_t m;
+  uint32_t src;
+  uint32_t* level;
+  uint32_t* visited;
+  uint32_t* fbits[3];
+  FrontierQueues fq;
+  BfsCtl* ctl;
+  uint32_t heavy;
+  uint32_t tile;
+  float alpha, beta;
+  uint32_t max_levels;
+};
+
+__global__ void bfs_init(BfsArgs a) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t words = (a.n + 31) >> 5;
+  for (uint64_t v = tid; v < a.n; v += stride) a.level[v] = (v == a.src) ? 0u : kInf;
+  for (uint64_t w = tid; w < words; w += stride) {
+    const uint32_t bit = (w == (a.src >> 5)) ? (1u << (a.src & 31)) : 0u;
+    a.visited[w] = bit;
+    a.fbits[0][w] = bit;
+    a.fbits[1][w] = 0;
+    a.fbits[2][w] = 0;
+  }
+  if (tid == 0) {
+    const uint64_t b = a.offs[a.src], d = a.offs[a.src + 1] - b;
+    FrontierCounters& c = a.ctl->fc[0];
+    c.vertices = 1;
+    c.degree_sum = d;
+    if (d > 0) seed_vertex(a.fq, 0, c, a.src, d, a.heavy, a.tile);
+    a.ctl->reached = 1;
+    a.ctl->reached_deg = d;
+  }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) bfs_persistent(BfsArgs a) {
+  BfsCtl* ctl = a.ctl;
+  const unsigned nblocks = gridDim.x;
+  const uint64_t deadline = kernel_deadline();
+  const uint32_t lane = lane_id();
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  const uint32_t words = (a.n + 31) >> 5;
+  const bool can_pull = a.in_offs != nullptr;
+
+  // direction-optimisation state (bfsDirectionOpt.cpp:247-337), replicated
+  // identically in every thread
+  int64_t edges_to_check = (int64_t)a.m;
+  int pull = 0;
+  uint32_t old_items = 0;
+  unsigned long long my_scanned = 0;
+
+  for (uint32_t L = 0;; ++L) {
+    const int rd = L % 3, wr = (L + 1) % 3, cl = (L + 2) % 3;
+    FrontierCounters& cur = ctl->fc[rd];
+    FrontierCounters& nxt = ctl->fc[wr];
+    // counts can exceed capacity only after an overflow (error raised); clamp reads
+    const uint32_t q_light = min(cur.light, a.fq.light_cap);
+    const uint32_t q_tiles = min(cur.tiles, a.fq.tile_cap);
+    const uint32_t items = cur.vertices;
+    const unsigned long long scout = cur.degree_sum;
+    if (q_light == 0 && q_tiles == 0) break;
+    if (L >= a.max_levels) {
+      if (gtid == 0) raise_err(&ctl->err, kDevMaxRounds);
+      break;
+    }
+    // choose the direction for this level
+    if (can_pull) {
+      if (!pull) {
+        if ((double)scout > (double)edges_to_check / a.alpha) { pull = 1; old_items = 0; }
+      } else {
+        if (!(items >= old_items || items > a.n / a.beta)) pull = 0;
+      }
+    }
+    if (pull) old_items = items;
+    else edges_to_check -= (int64_t)scout;
+
+    if (gtid == 0) {
+      ctl->fc[cl] = FrontierCounters{};
+      ctl->levels = L + 1;
+      if (pull) ctl->pull_levels += 1;
+    }
+    uint32_t* fb_rd = a.fbits[rd];
+    uint32_t* fb_wr = a.fbits[wr];
+    uint32_t* fb_cl = a.fbits[cl];
+    for (uint64_t w = gtid; w < words; w += gthreads) fb_cl[w] = 0;
+    const uint32_t next_level = L + 1;
+
+    // discovery: all lanes call with their candidate
+    auto discover = [&](bool cand, uint32_t u) {
+      bool disc = false;
+      if (cand) {
+        const uint32_t bit = 1u << (u & 31);
+        if (!(a.visited[u >> 5] & bit)) {
+          const uint32_t old = atomicOr(&a.visited[u >> 5], bit);
+          disc = !(old & bit);
+        }
+        if (disc) {
+          a.level[u] = next_level;
+          atomicOr(&fb_wr[u >> 5], bit);
+        }
+      }
+      push_discovered(a.fq, (L + 1) & 1, nxt, disc, u, a.offs, a.heavy, a.tile, &ctl->err);
+    };
+
+    if (!pull) {
+      const uint32_t* qin = a.fq.light[L & 1];
+      const uint2* tin = a.fq.tiles[L & 1];
+      // light vertices, 32 per warp grab
+      for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&cur.light_work, 32u);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= q_light) break;
+        const uint32_t idx = base + lane;
+        uint64_t b = 0;
+        uint32_t d = 0;
+        if (idx < q_light) {
+          const uint32_t v = qin[idx];
+          b = ldg(a.offs + v);
+          d = (uint32_t)(ldg(a.offs + v + 1) - b);
+        }
+        my_scanned += d;
+        warp_expand(b, d, 0u, [&](bool valid, uint64_t e, uint32_t, uint32_t) {
+          const uint32_t u = valid ? ldg(a.col + e) : 0u;
+          discover(valid, u);
+        });
+      }
+      // heavy vertices' edge tiles, one tile per warp grab
+      for (;;) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(&cur.tile_work, 1u);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= q_tiles) break;
+        const uint2 tv = tin[t];
+        const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
+        const uint64_t b = vb + (uint64_t)tv.y * a.tile;
+        const uint64_t e_end = min(ve, b + a.tile);
+        if (lane == 0) my_scanned += e_end - b;
+        for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
+          const uint64_t e = e0 + lane;
+          const bool valid = e < e_end;
+          const uint32_t u = valid ? ldg(a.col + e) : 0u;
+          discover(valid, u);
+        }
+      }
+    } else {
+      // bottom-up over all vertices; warp-uniform trip count
+      for (uint64_t base = gtid - lane; base < a.n; base += gthreads) {
+        const uint64_t u64 = base + lane;
+        bool found = false;
+        uint32_t u = (uint32_t)u64;
+        if (u64 < a.n) {
+          const uint32_t bit = 1u << (u & 31);
+          if (!(a.visited[u >> 5] & bit)) {
+            const uint64_t b = ldg(a.in_offs + u), e = ldg(a.in_offs + u + 1);
+            uint64_t i = b;
+            for (; i < e; ++i) {
+              const uint32_t p = ldg(a.in_col + i);
+              if (fb_rd[p >> 5] & (1u << (p & 31))) { found = true; ++i; break; }
+            }
+            my_scanned += i - b;
+          }
+        }
+        bool disc = false;
+        if (found) {
+          const uint32_t bit = 1u << (u & 31);
+          const uint32_t old = atomicOr(&a.visited[u >> 5], bit);
+          disc = !(old & bit);
+          if (disc) {
+            a.level[u] = next_level;
+            atomicOr(&fb_wr[u >> 5], bit);
+          }
+        }
+        push_discovered(a.fq, (L + 1) & 1, nxt, disc, u, a.offs, a.heavy, a.tile, &ctl->err);
+      }
+    }
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    if (gtid == 0) {
+      ctl->reached += nxt.vertices;
+      ctl->reached_deg += nxt.degree_sum;
+    }
+  }
+  my_scanned = warp_sum(my_scanned);
+  if (lane == 0 && my_scanned) atomicAdd(&ctl->scanned, my_scanned);
+}
+
+}  // namespace
+
+int run_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats, cudaStream_t s,
+            void* scratch, size_t scratch_bytes) {
+  const gb_tuning t = effective_tuning(g);
+  const uint32_t n = g->n;
+  const uint32_t words = (n + 31) / 32;
+  const bool out_dev = is_device_ptr(level_out);
+  FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
+  size_t need = carve_size<BfsCtl>(1) + 4 * carve_size<uint32_t>(words) + fl.bytes +
+                (out_dev ? 0 : carve_size<uint32_t>(n));
+  void* base = scratch;
+  if (!base) {
+    int st = ws_reserve(g, need, s);
+    if (st != GB_OK) return st;
+    base = g->ws;
+  } else if (scratch_bytes < need) {
+    GB_FAIL(GB_ERR_CAPACITY, "gb_bfs: scratch of %zu bytes, need %zu", scratch_bytes, need);
+  }
+  Carver cv(base);
+  BfsArgs a{};
+  a.ctl = cv.take<BfsCtl>(1);
+  a.visited = cv.take<uint32_t>(words);
+  for (int i = 0; i < 3; ++i) a.fbits[i] = cv.take<uint32_t>(words);
+  a.fq = carve_frontier(cv, fl);
+  a.level = out_dev ? level_out : cv.take<uint32_t>(n);
+  a.offs = g->offs;
+  a.col = g->col;
+  const bool allow_pull = t.direction_opt != 2;
+  if (allow_pull && g->symmetric) {
+    a.in_offs = g->offs;
+    a.in_col = g->col;
+  } else if (allow_pull && g->t_offs) {
+    a.in_offs = g->t_offs;
+    a.in_col = g->t_col;
+  }
+  a.n = n;
+  a.m = g->m;
+  a.src = src;
+  a.heavy = t.heavy_degree;
+  a.tile = t.tile_edges;
+  a.alpha = t.do_alpha;
+  a.beta = t.do_beta;
+  a.max_levels = n + 1;
+  GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(BfsCtl), s));
+  bfs_init<<<g->sm_count * 4, 256, 0, s>>>(a);
+  GB_CUDA(cudaGetLastError());
+  const void* kfn = reinterpret_cast<const void*>(&bfs_persistent<256>);
+  const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
+  if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_bfs: cannot size cooperative grid");
+  void* args[] = {&a};
+  GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, args, 0, s));
+  int* pin = static_cast<int*>(g->pinned);
+  GB_CUDA(cudaMemcpyAsync(pin, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (stats) {
+    BfsCtl* hc = reinterpret_cast<BfsCtl*>(static_cast<char*>(g->pinned) + 256);
+    GB_CUDA(cudaMemcpyAsync(hc, a.ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    stats->vertices_reached = hc->reached;
+    stats->edges_reached = hc->reached_deg;
+    stats->edges_scanned = hc->scanned;
+    stats->relaxations = hc->reached;
+    stats->rounds = hc->levels;
+    stats->pull_rounds = hc->pull_levels;
+    stats->buckets = 0;
+    stats->launches = 2;
+    stats->residual = 0;
+  }
+  if (!out_dev) {
+    int st = copy_out(level_out, a.level, sizeof(uint32_t) * n, s);
+    if (st != GB_OK) return st;
+  }
+  if (stats || !out_dev) {
+    GB_CUDA(cudaStreamSynchronize(s));
+    if (*pin) return dev_err_status(*pin, "gb_bfs");
+  }
+  return GB_OK;
+}
+
+}  // namespace gb
+
+extern "C" int gb_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats, void* stream) {
+  gb::clear_error();
+  if (!g || !level_out) GB_FAIL(GB_ERR_ARG, "gb_bfs: null argument");
+  if (src >= g->n) GB_FAIL(GB_ERR_ARG, "gb_bfs: source %u >= n %u", src, g->n);
+  GB_CUDA(cudaSetDevice(g->device));
+  return gb::run_bfs(g, src, level_out, stats, static_cast<cudaStream_t>(stream), nullptr, 0);
+}

@@ -1,0 +1,289 @@
+// Connected components with minimum-id labels.
+//
+// Reference semantics: lonestar/analytics/cpu/connected-components/
+// ConnectedComponents.cpp:183-230 (LabelPropAlgo: comp_current starts at the
+// vertex id, min-labels propagate over edges until nothing changes), init
+// :1162-1172, verify :1046-1072.  LabelProp converges to the minimum vertex id
+// of each component; every algorithm here produces exactly that labelling.
+//
+// Algorithms (one cooperative persistent launch each, rounds separated by the
+// bounded grid barrier):
+//   GB_CC_LABELPROP  label propagation with pointer jumping: per round, every
+//                    edge (v,u) hooks the larger of (p[v], p[u]) under the
+//                    smaller with atomicMin, then every vertex jumps to its
+//                    root.  p[x] <= x always holds and sum(p) strictly drops
+//                    while anything changes, so it terminates with p = min id.
+//   GB_CC_UNIONFIND  one sweep of lock-free union-find (larger root linked
+//                    under the smaller with atomicCAS, path halving), then a
+//                    compression sweep.  Same labels.
+//   GB_CC_AFFOREST   neighbour sampling (first 2 arcs of every vertex), a
+//                    compression, detection of the most frequent root, then
+//                    union-find only over vertices outside that component.
+// On a symmetric graph each undirected edge is processed once (u > v); on a
+// directed graph every arc is processed, giving weakly connected components.
+
+#include "device_common.cuh"
+#include "device_graph.cuh"
+#include "sweep.cuh"
+
+namespace gb {
+
+namespace {
+
+struct CcCtl {
+  GridBar bar;
+  int err;
+  uint32_t changed[3];
+  uint32_t rounds;
+  uint32_t giant;
+  uint32_t pad;
+  unsigned long long scanned;
+};
+
+struct CcArgs {
+  const uint64_t* __restrict__ offs;
+  const uint32_t* __restrict__ col;
+  uint32_t n;
+  int half;  // process only u > v (symmetric graph)
+  uint32_t* p;
+  SweepSched sched;
+  CcCtl* ctl;
+  uint32_t* hist;  // Afforest root histogram sample
+  uint32_t max_rounds;
+};
+
+__global__ void cc_init(uint32_t* p, uint32_t n) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = tid; v < n; v += stride) p[v] = (uint32_t)v;
+}
+
+__device__ __forceinline__ uint32_t find_root(uint32_t* p, uint32_t x) {
+  uint32_t px = p[x];
+  while (px != x) {
+    const uint32_t ppx = p[px];
+    if (ppx != px) p[x] = ppx;  // path halving (benign race: ancestors only)
+    x = px;
+    px = ppx;
+  }
+  return x;
+}
+
+// Link the trees of a and b: larger root goes under the smaller (ECL-CC style).
+__device__ __forceinline__ void link(uint32_t* p, uint32_t a, uint32_t b) {
+  uint32_t ra = find_root(p, a), rb = find_root(p, b);
+  for (int guard = 0; ra != rb && guard < (1 << 20); ++guard) {
+    if (ra < rb) {
+      const uint32_t ret = atomicCAS(&p[rb], rb, ra);
+      if (ret == rb) break;
+      rb = find_root(p, ret);
+    } else {
+      const uint32_t ret = atomicCAS(&p[ra], ra, rb);
+      if (ret == ra) break;
+      ra = find_root(p, ret);
+    }
+  }
+}
+
+__device__ __forceinline__ void compress_all(CcArgs& a, uint64_t gtid, uint64_t gthreads) {
+  for (uint64_t v = gtid; v < a.n; v += gthreads) {
+    uint32_t x = a.p[v];
+    while (x != a.p[x]) x = a.p[x];
+    a.p[v] = x;
+  }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
+  CcCtl* ctl = a.ctl;
+  const uint64_t deadline = kernel_deadline();
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const uint32_t lane = lane_id();
+  unsigned long long my_scanned = 0;
+  for (uint32_t r = 0;; ++r) {
+    if (r >= a.max_rounds) {
+      if (gtid == 0) raise_err(&ctl->err, kDevMaxRounds);
+      break;
+    }
+    uint32_t* changed = &ctl->changed[r % 3];
+    if (gtid == 0) ctl->changed[(r + 1) % 3] = 0;
+    bool my_change = false;
+    auto hook = [&](bool valid, uint32_t v, uint32_t u) {
+      if (valid && (!a.half || u > v)) {
+        const uint32_t pv = a.p[v], pu = a.p[u];
+        if (pv != pu) {
+          const uint32_t hi = max(pv, pu), lo = min(pv, pu);
+          if (lo < a.p[hi]) {
+            atomicMin(&a.p[hi], lo);
+            my_change = true;
+          }
+        }
+      }
+    };
+    sweep_all(
+        a.offs, a.n, a.sched, gwarp, nwarps,
+        [&](bool valid, uint64_t e, uint32_t, uint32_t v) { hook(valid, v, valid ? ldg(a.col + e) : 0u); },
+        [&](uint32_t, bool, bool) {},
+        [&](uint32_t v, uint64_t b, uint64_t e) {
+          if (lane == 0) my_scanned += e - b;
+          for (uint64_t i = b + lane; i < e; i += 32) hook(true, v, ldg(a.col + i));
+        });
+    if (__any_sync(kFull, my_change) && lane == 0) atomicOr(changed, 1u);
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    compress_all(a, gtid, gthreads);
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    if (gtid == 0) ctl->rounds = r + 1;
+    if (*reinterpret_cast<volatile uint32_t*>(changed) == 0) break;
+  }
+  my_scanned = warp_sum(my_scanned);
+  if (lane == 0 && my_scanned) atomicAdd(&ctl->scanned, my_scanned);
+}
+
+// Union-find: mode 0 = all arcs; mode 1 = Afforest (sample, then the rest).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) cc_unionfind(CcArgs a, int afforest) {
+  CcCtl* ctl = a.ctl;
+  const uint64_t deadline = kernel_deadline();
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const uint32_t lane = lane_id();
+  constexpr uint32_t kSamples = 2;
+  uint32_t giant = 0xFFFFFFFFu;
+  if (afforest) {
+    // 1. neighbour sampling: link every vertex with its first kSamples arcs
+    for (uint64_t v = gtid; v < a.n; v += gthreads) {
+      const uint64_t b = ldg(a.offs + v), e = ldg(a.offs + v + 1);
+      for (uint64_t i = b; i < e && i < b + kSamples; ++i) link(a.p, (uint32_t)v, ldg(a.col + i));
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    compress_all(a, gtid, gthreads);
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    // 2. most frequent root among 1024 evenly spaced vertices
+    if (blockIdx.x == 0) {
+      __shared__ uint32_t s_root[1024];
+      __shared__ uint32_t s_cnt[1024];
+      for (uint32_t i = threadIdx.x; i < 1024; i += BLOCK) {
+        const uint32_t v = (uint32_t)(((uint64_t)i * a.n) >> 10);
+        s_root[i] = a.p[v];
+      }
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < 1024; i += BLOCK) {
+        uint32_t c = 0;
+        for (uint32_t j = 0; j < 1024; ++j) c += s_root[j] == s_root[i];
+        s_cnt[i] = c;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        uint32_t best = s_root[0], bestc = 0;
+        for (uint32_t i = 0; i < 1024; ++i)
+          if (s_cnt[i] > bestc) { bestc = s_cnt[i]; best = s_root[i]; }
+        ctl->giant = best;
+      }
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    giant = *reinterpret_cast<volatile uint32_t*>(&ctl->giant);
+  }
+  unsigned long long my_scanned = 0;
+  // 3. union-find over all remaining arcs (Afforest: skip vertices already in
+  //    the giant component and the arcs already sampled)
+  auto skip_vertex = [&](uint32_t v) { return afforest && a.p[v] == giant; };
+  sweep_all(
+      a.offs, a.n, a.sched, gwarp, nwarps,
+      [&](bool valid, uint64_t e, uint32_t, uint32_t v) {
+        if (!valid) return;
+        const uint32_t u = ldg(a.col + e);
+        if (a.half && !afforest && u < v) return;
+        if (afforest && (skip_vertex(v) || e < ldg(a.offs + v) + kSamples)) return;
+        link(a.p, v, u);
+      },
+      [&](uint32_t, bool, bool) {},
+      [&](uint32_t v, uint64_t b, uint64_t e) {
+        if (afforest && skip_vertex(v)) return;
+        if (lane == 0) my_scanned += e - b;
+        const uint64_t b0 = ldg(a.offs + v);
+        for (uint64_t i = b + lane; i < e; i += 32) {
+          const uint32_t u = ldg(a.col + i);
+          if (a.half && !afforest && u < v) continue;
+          if (afforest && i < b0 + kSamples) continue;
+          link(a.p, v, u);
+        }
+      });
+  if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+  compress_all(a, gtid, gthreads);
+  if (gtid == 0) ctl->rounds = 1;
+  my_scanned = warp_sum(my_scanned);
+  if (lane == 0 && my_scanned) atomicAdd(&ctl->scanned, my_scanned);
+}
+
+}  // namespace
+
+int run_cc(gb_graph* g, int algo, uint32_t* label_out, gb_stats* stats, cudaStream_t s) {
+  if (algo < 0 || algo > 2) GB_FAIL(GB_ERR_ARG, "gb_cc: unknown algo %d", algo);
+  if (algo == GB_CC_AFFOREST && !g->symmetric)
+    GB_FAIL(GB_ERR_UNSUPPORTED, "gb_cc: Afforest needs a symmetric graph (it skips the giant component's arcs)");
+  const gb_tuning t = effective_tuning(g);
+  const uint32_t n = g->n;
+  const bool out_dev = is_device_ptr(label_out);
+  SweepSched sched;
+  int st = ensure_sweep_schedule(g, t.heavy_degree, t.tile_edges, s, &sched);
+  if (st != GB_OK) return st;
+  const size_t need = carve_size<CcCtl>(1) + carve_size<uint32_t>(1024) + (out_dev ? 0 : carve_size<uint32_t>(n));
+  st = ws_reserve(g, need, s);
+  if (st != GB_OK) return st;
+  Carver cv(g->ws);
+  CcArgs a{};
+  a.ctl = cv.take<CcCtl>(1);
+  a.hist = cv.take<uint32_t>(1024);
+  a.p = out_dev ? label_out : cv.take<uint32_t>(n);
+  a.offs = g->offs;
+  a.col = g->col;
+  a.n = n;
+  a.half = g->symmetric ? 1 : 0;
+  a.sched = sched;
+  a.max_rounds = 1u << 20;
+  GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(CcCtl), s));
+  cc_init<<<g->sm_count * 4, 256, 0, s>>>(a.p, n);
+  GB_CUDA(cudaGetLastError());
+  const void* kfn = algo == GB_CC_LABELPROP ? reinterpret_cast<const void*>(&cc_labelprop<256>)
+                                            : reinterpret_cast<const void*>(&cc_unionfind<256>);
+  const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
+  if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_cc: cannot size cooperative grid");
+  int aff = algo == GB_CC_AFFOREST ? 1 : 0;
+  void* args_lp[] = {&a};
+  void* args_uf[] = {&a, &aff};
+  GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, algo == GB_CC_LABELPROP ? args_lp : args_uf, 0, s));
+  int* pin = static_cast<int*>(g->pinned);
+  GB_CUDA(cudaMemcpyAsync(pin, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (stats) {
+    CcCtl* hc = reinterpret_cast<CcCtl*>(static_cast<char*>(g->pinned) + 256);
+    GB_CUDA(cudaMemcpyAsync(hc, a.ctl, sizeof(CcCtl), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    *stats = gb_stats{};
+    stats->vertices_reached = n;
+    stats->edges_reached = g->m;
+    stats->edges_scanned = hc->scanned;
+    stats->rounds = hc->rounds;
+    stats->launches = 2;
+  }
+  if (!out_dev) {
+    st = copy_out(label_out, a.p, sizeof(uint32_t) * n, s);
+    if (st != GB_OK) return st;
+  }
+  if (stats || !out_dev) {
+    GB_CUDA(cudaStreamSynchronize(s));
+    if (*pin) return dev_err_status(*pin, "gb_cc");
+  }
+  return GB_OK;
+}
+
+}  // namespace gb
+
+extern "C" int gb_cc(gb_graph* g, int algo, uint32_t* label_out, gb_stats* stats, void* stream) {
+  gb::clear_error();
+  if (!g || !label_out) GB_FAIL(GB_ERR_ARG, "gb_cc: null argument");
+  GB_CUDA(cudaSetDevice(g->device));
+  return gb::run_cc(g, algo, label_out, stats, static_cast<cudaStream_t>(stream));
+}

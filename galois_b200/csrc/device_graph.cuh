@@ -1,0 +1,102 @@
+// The device mirror of an LC_CSR_Graph (libgalois/include/galois/graphs/
+// LC_CSR_Graph.h:133-178) plus the per-handle scratch workspace.
+//
+// Layout in HBM (all arrays 256-byte aligned by cudaMalloc):
+//   offs   uint64[n+1]  begin offsets (the LC end offsets with a leading 0)
+//   col    uint32[m]    destinations, adjacency sorted ascending
+//   w      uint32[m]    integer weights (SSSP), optional
+//   wf     float[m]     float weights (PPR), optional
+//   t_*    the same for the transposed graph (in-edges), built on demand,
+//          with t_emap uint64[m] mapping each in-arc to its out-arc index.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "gb_internal.h"
+
+struct gb_graph {
+  int device = 0;
+  uint32_t n = 0;
+  uint64_t m = 0;
+  int symmetric = 0;
+  int sm_count = 148;
+  uint64_t* offs = nullptr;
+  uint32_t* col = nullptr;
+  uint32_t* w = nullptr;
+  float* wf = nullptr;
+  // transposed (in-edge) CSR
+  uint64_t* t_offs = nullptr;
+  uint32_t* t_col = nullptr;
+  float* t_wf = nullptr;
+  uint64_t* t_emap = nullptr;
+  // cached per-graph derived arrays
+  uint32_t* outdeg_of_stored = nullptr;  // PageRank nout (in-degree counts of the stored graph)
+  float* colsum = nullptr;               // PPR column sums of wf by source
+  uint32_t max_degree = 0;
+  // all-vertex sweep schedule (sweep.cuh), cached per (heavy, tile)
+  uint2* sweep_tiles = nullptr;
+  uint32_t* sweep_heavy_list = nullptr;
+  uint32_t sweep_ntiles = 0;
+  uint32_t sweep_nheavy = 0;
+  uint32_t sweep_heavy = 0;
+  uint32_t sweep_tile = 0;
+  // scratch workspace, grown on demand
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  // pinned host staging for small readbacks
+  void* pinned = nullptr;
+  gb_tuning tuning{};
+};
+
+namespace gb {
+
+// status helpers
+int cuda_fail(cudaError_t e, const char* what);
+#define GB_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return ::gb::cuda_fail(_e, #call); \
+  } while (0)
+
+bool is_device_ptr(const void* p);
+// Ensure at least `bytes` of workspace; returns GB_OK or an error status.
+int ws_reserve(gb_graph* g, size_t bytes, cudaStream_t stream);
+// Bump-carve helper over the workspace.
+struct Carver {
+  char* base;
+  size_t off = 0;
+  explicit Carver(void* b) : base(static_cast<char*>(b)) {}
+  template <class T>
+  T* take(size_t count) {
+    off = (off + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += count * sizeof(T);
+    return p;
+  }
+};
+template <class T>
+inline size_t carve_size(size_t count) {
+  return ((count * sizeof(T)) + 255) & ~size_t(255);
+}
+
+// Resolved tuning with defaults filled in.
+gb_tuning effective_tuning(const gb_graph* g);
+
+// Number of CTAs for a cooperative launch of `kernel` with `threads` threads.
+int coop_grid(const gb_graph* g, const void* kernel, int threads, size_t smem,
+              uint32_t blocks_per_sm_cap);
+
+// Map a device error word to a status (and message).
+int dev_err_status(int code, const char* what);
+
+// Copy `count` elements of device data to a caller buffer (host or device).
+int copy_out(void* dst, const void* src_dev, size_t bytes, cudaStream_t stream);
+// Upload caller data (host or device) into a device buffer.
+int copy_in(void* dst_dev, const void* src, size_t bytes, cudaStream_t stream);
+
+int ensure_transpose(gb_graph* g, cudaStream_t stream);
+
+}  // namespace gb

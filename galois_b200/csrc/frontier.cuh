@@ -1,0 +1,101 @@
+// Device frontier queues: the B200 replacement for Galois' InsertBag of
+// vertices / edge tiles (BFS_SSSP.h:81-131, bfs.cpp:244-293) and libgpu's
+// Worklist2 (libgpu/include/worklist.h:410-510).
+//
+// A frontier is two queues: `light` holds vertices whose degree is at most
+// `heavy` (expanded 32 at a time by one warp), `tiles` holds (vertex, k) pairs
+// naming the k-th run of `tile` arcs of a heavier vertex (one warp per tile).
+// Degree binning happens once, when a vertex is discovered.
+#pragma once
+
+#include "device_common.cuh"
+#include "device_graph.cuh"
+
+namespace gb {
+
+struct FrontierCounters {
+  uint32_t light;       // entries in the light queue
+  uint32_t tiles;       // entries in the tile queue
+  uint32_t vertices;    // vertices discovered into this frontier (any degree)
+  uint32_t light_work;  // dynamic work-distribution cursors
+  uint32_t tile_work;
+  uint32_t pad;
+  unsigned long long degree_sum;  // sum of out-degrees of discovered vertices
+};
+
+struct FrontierQueues {
+  uint32_t* light[2];
+  uint2* tiles[2];
+  uint32_t light_cap;
+  uint32_t tile_cap;
+};
+
+struct FrontierLayout {
+  uint32_t light_cap;
+  uint32_t tile_cap;
+  size_t bytes;
+};
+
+inline FrontierLayout frontier_layout(uint32_t n, uint64_t m, uint32_t heavy, uint32_t tile) {
+  FrontierLayout l;
+  l.light_cap = n;
+  uint64_t tc = m / tile + m / ((uint64_t)heavy + 1) + 2;
+  if (tc > 0xFFFFFFF0ull) tc = 0xFFFFFFF0ull;
+  l.tile_cap = (uint32_t)tc;
+  l.bytes = 2 * carve_size<uint32_t>(l.light_cap) + 2 * carve_size<uint2>(l.tile_cap);
+  return l;
+}
+
+inline FrontierQueues carve_frontier(Carver& cv, const FrontierLayout& l) {
+  FrontierQueues q;
+  q.light[0] = cv.take<uint32_t>(l.light_cap);
+  q.light[1] = cv.take<uint32_t>(l.light_cap);
+  q.tiles[0] = cv.take<uint2>(l.tile_cap);
+  q.tiles[1] = cv.take<uint2>(l.tile_cap);
+  q.light_cap = l.light_cap;
+  q.tile_cap = l.tile_cap;
+  return q;
+}
+
+// Single-thread seeding of a source vertex into queue buffer qb.
+__device__ __forceinline__ void seed_vertex(const FrontierQueues& q, int qb, FrontierCounters& c,
+                                            uint32_t v, uint64_t d, uint32_t heavy, uint32_t tile) {
+  if (d <= heavy) {
+    q.light[qb][c.light++] = v;
+  } else {
+    const uint32_t nt = (uint32_t)((d + tile - 1) / tile);
+    for (uint32_t k = 0; k < nt && c.tiles < q.tile_cap; ++k) q.tiles[qb][c.tiles++] = make_uint2(v, k);
+  }
+}
+
+// Warp-collective: append every lane's discovered vertex `u` (disc == true)
+// into queue buffer qb, binned by degree; zero-degree vertices are counted but
+// not queued (they have nothing to expand).  All 32 lanes must call.
+__device__ __forceinline__ void push_discovered(const FrontierQueues& q, int qb, FrontierCounters& c,
+                                                bool disc, uint32_t u, const uint64_t* __restrict__ offs,
+                                                uint32_t heavy, uint32_t tile, int* err) {
+  uint64_t d = 0;
+  if (disc) d = __ldg(offs + u + 1) - __ldg(offs + u);
+  const bool light = disc && d > 0 && d <= heavy;
+  const bool hv = disc && d > heavy;
+  warp_push(light, u, q.light[qb], &c.light, q.light_cap, err);
+  const unsigned hmask = __ballot_sync(kFull, hv);
+  if (hmask) {
+    const uint32_t nt = hv ? (uint32_t)((d + tile - 1) / tile) : 0u;
+    const uint32_t first = warp_reserve(nt, &c.tiles);
+    for (uint32_t k = 0; k < nt; ++k) {
+      if (first + k < q.tile_cap) q.tiles[qb][first + k] = make_uint2(u, k);
+      else raise_err(err, kDevOverflow);
+    }
+  }
+  const unsigned dmask = __ballot_sync(kFull, disc);
+  if (dmask) {
+    const unsigned long long ds = warp_sum((unsigned long long)d);
+    if (lane_id() == 0) {
+      atomicAdd(&c.vertices, (uint32_t)__popc(dmask));
+      if (ds) atomicAdd(&c.degree_sum, ds);
+    }
+  }
+}
+
+}  // namespace gb

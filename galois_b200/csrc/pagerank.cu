@@ -1,0 +1,531 @@
+// PageRank: pull-topological, pull-residual and residual-push.
+//
+// Reference semantics (lonestar/analytics/cpu/pagerank):
+//   pull-topological  PageRank-pull.cpp:196-251 over the TRANSPOSED graph:
+//                     value = 1/n; nout = in-degree of the stored graph
+//                     (computeOutDeg :90-122); per iteration
+//                     value[v] = alpha * sum_{u in edges(v)} value[u]/nout[u]
+//                                + (1-alpha)/n,
+//                     stop when sum |delta| <= tol or at maxIterations.
+//                     The CPU code updates in place (schedule-dependent); the
+//                     device runs the Jacobi form, which the FP64 oracle
+//                     restates.
+//   pull-residual     PageRank-pull.cpp:132-190 (delta/residual rounds).
+//   residual push     PageRank-push.cpp:103-188 (Sync): value 0, residual
+//                     1-alpha; active vertices over tol absorb their residual
+//                     and push residual*alpha/outdeg along out-edges; a
+//                     vertex is activated when its residual crosses tol.
+//
+// B200 design: one cooperative persistent launch per solve.  Pull iterations
+// use the cached all-vertex sweep schedule (sweep.cuh): 32 consecutive
+// vertices per warp with a segmented shuffle reduction per owner vertex,
+// heavy vertices as tiles whose partial sums meet in an accumulator, a
+// contribution array c[u] = value[u]/nout[u] (SoA, double-buffered) so each
+// arc costs one 4-byte column read and one 4-byte gather, and the L1 change
+// reduced in fp64.  Residual push reuses the frontier queues (frontier.cuh).
+
+#include "device_common.cuh"
+#include "device_graph.cuh"
+#include "frontier.cuh"
+#include "sweep.cuh"
+
+#include <cstring>
+
+namespace gb {
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kWarps = kBlock / 32;
+
+struct PrCtl {
+  GridBar bar;
+  int err;
+  uint32_t iters;
+  double l1[3];
+  uint32_t linf[3];  // max |delta| as float bits (non-negative floats order as uints)
+  uint32_t active[3];
+  uint32_t pad;
+  FrontierCounters fc[3];
+  unsigned long long pushes;
+};
+
+struct PrArgs {
+  const uint64_t* __restrict__ offs;
+  const uint32_t* __restrict__ col;
+  const uint32_t* __restrict__ nout;
+  uint32_t n;
+  float alpha;
+  float base;
+  float tol;
+  uint32_t max_iter;
+  float init;  // initial rank (1/n for the lonestar app)
+  int linf;    // 1: stop on max |delta| (python/galois/_pagerank.pyx:114-139)
+  float* value;
+  float* c[2];
+  float* acc;
+  SweepSched sched;
+  PrCtl* ctl;
+  // residual variants
+  float* residual;
+  float* delta;
+  uint32_t* active[2];
+  uint32_t* stamp;
+  FrontierQueues fq;
+  uint32_t heavy, tile;
+};
+
+__global__ void count_nout(const uint32_t* __restrict__ col, uint64_t m, uint32_t* nout) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = tid; e < m; e += stride) atomicAdd(&nout[col[e]], 1u);
+}
+
+__global__ void pr_pull_init(PrArgs a) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const float init = a.init;  // 1/n: PageRank-pull.cpp:62
+  for (uint64_t v = tid; v < a.n; v += stride) {
+    a.value[v] = init;
+    const uint32_t k = a.nout[v];
+    a.c[0][v] = k ? init / (float)k : 0.f;
+    a.acc[v] = 0.f;
+  }
+}
+
+// Segmented (by owner lane) warp reduction of x; returns true on the lane
+// that heads its segment, which then holds the segment's sum.
+__device__ __forceinline__ bool seg_reduce(bool valid, uint32_t owner, float& x) {
+  const uint32_t lane = lane_id();
+  const uint32_t key = valid ? owner : 0xFFFFFFFFu;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const float y = __shfl_down_sync(kFull, x, off);
+    const uint32_t k2 = __shfl_down_sync(kFull, key, off);
+    if (lane + off < 32 && k2 == key) x += y;
+  }
+  const uint32_t kprev = __shfl_up_sync(kFull, key, 1);
+  return valid && (lane == 0 || kprev != key);
+}
+
+__global__ void __launch_bounds__(kBlock) pr_pull_persistent(PrArgs a) {
+  __shared__ float s_acc[kWarps][32];
+  PrCtl* ctl = a.ctl;
+  const uint64_t deadline = kernel_deadline();
+  const uint64_t gtid = blockIdx.x * (uint64_t)kBlock + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * kBlock;
+  const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  s_acc[wib][lane] = 0.f;
+  __syncwarp();
+  for (uint32_t it = 0;; ++it) {
+    const float* __restrict__ c_in = a.c[it & 1];
+    float* __restrict__ c_out = a.c[(it + 1) & 1];
+    if (gtid == 0) {
+      ctl->l1[(it + 1) % 3] = 0.0;
+      ctl->linf[(it + 1) % 3] = 0u;
+    }
+    double my_l1 = 0.0;
+    float my_max = 0.f;
+    auto finish = [&](uint32_t v, float sum) {
+      const float value = sum * a.alpha + a.base;  // PageRank-pull.cpp:222
+      const float old = a.value[v];
+      a.value[v] = value;
+      const uint32_t k = a.nout[v];
+      c_out[v] = k ? value / (float)k : 0.f;
+      my_l1 += (double)fabsf(value - old);
+      my_max = fmaxf(my_max, fabsf(value - old));
+    };
+    sweep_all(
+        a.offs, a.n, a.sched, gwarp, nwarps,
+        [&](bool valid, uint64_t e, uint32_t owner, uint32_t) {
+          float x = valid ? c_in[ldg(a.col + e)] : 0.f;
+          if (seg_reduce(valid, owner, x)) s_acc[wib][owner] += x;
+          __syncwarp();
+        },
+        [&](uint32_t v, bool valid, bool heavy) {
+          const float sum = s_acc[wib][lane];
+          s_acc[wib][lane] = 0.f;
+          __syncwarp();
+          if (valid && !heavy) finish(v, sum);
+        },
+        [&](uint32_t v, uint64_t b, uint64_t e) {
+          float s = 0.f;
+          for (uint64_t i = b + lane; i < e; i += 32) s += c_in[ldg(a.col + i)];
+          s = warp_sum(s);
+          if (lane == 0) atomicAdd(&a.acc[v], s);
+        });
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    for (uint64_t i = gtid; i < a.sched.nheavy; i += gthreads) {
+      const uint32_t v = a.sched.heavy_list[i];
+      const float sum = a.acc[v];
+      a.acc[v] = 0.f;
+      finish(v, sum);
+    }
+    my_l1 = warp_sum(my_l1);
+    const uint32_t mbits = __reduce_max_sync(kFull, __float_as_uint(my_max));
+    if (lane == 0 && my_l1 != 0.0) atomicAdd(&ctl->l1[it % 3], my_l1);
+    if (lane == 0 && mbits != 0u) atomicMax(&ctl->linf[it % 3], mbits);
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    const double l1 = a.linf ? (double)__uint_as_float(*reinterpret_cast<volatile uint32_t*>(&ctl->linf[it % 3]))
+                             : *reinterpret_cast<volatile double*>(&ctl->l1[it % 3]);
+    if (gtid == 0) ctl->iters = it + 1;
+    if (l1 <= (double)a.tol || it + 1 >= a.max_iter) break;  // PageRank-pull.cpp:238-243
+  }
+}
+
+// ---- pull-residual (PageRank-pull.cpp:132-190) ------------------------------
+__global__ void pr_resid_init(PrArgs a) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = tid; v < a.n; v += stride) {
+    a.value[v] = 0.f;
+    a.delta[v] = 0.f;
+    a.residual[v] = 1.0f - a.alpha;  // INIT_RESIDUAL, PageRank-constants.h:33
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) pr_pull_residual_persistent(PrArgs a) {
+  __shared__ float s_acc[kWarps][32];
+  PrCtl* ctl = a.ctl;
+  const uint64_t deadline = kernel_deadline();
+  const uint64_t gtid = blockIdx.x * (uint64_t)kBlock + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * kBlock;
+  const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  s_acc[wib][lane] = 0.f;
+  __syncwarp();
+  for (uint32_t it = 0;; ++it) {
+    if (gtid == 0) ctl->active[(it + 1) % 3] = 0;
+    uint32_t my_accum = 0;
+    for (uint64_t v = gtid; v < a.n; v += gthreads) {
+      a.delta[v] = 0.f;
+      const float r = a.residual[v];
+      if (r > a.tol) {
+        a.residual[v] = 0.f;
+        a.value[v] += r;
+        const uint32_t k = a.nout[v];
+        if (k > 0) {
+          a.delta[v] = r * a.alpha / (float)k;
+          ++my_accum;
+        }
+      }
+    }
+    my_accum = __reduce_add_sync(kFull, my_accum);
+    if (lane == 0 && my_accum) atomicAdd(&ctl->active[it % 3], my_accum);
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    auto finish = [&](uint32_t v, float sum) {
+      if (sum > 0.f) a.residual[v] = sum;
+    };
+    sweep_all(
+        a.offs, a.n, a.sched, gwarp, nwarps,
+        [&](bool valid, uint64_t e, uint32_t owner, uint32_t) {
+          float x = 0.f;
+          if (valid) {
+            const float d = a.delta[ldg(a.col + e)];
+            x = d > 0.f ? d : 0.f;
+          }
+          if (seg_reduce(valid, owner, x)) s_acc[wib][owner] += x;
+          __syncwarp();
+        },
+        [&](uint32_t v, bool valid, bool heavy) {
+          const float sum = s_acc[wib][lane];
+          s_acc[wib][lane] = 0.f;
+          __syncwarp();
+          if (valid && !heavy) finish(v, sum);
+        },
+        [&](uint32_t v, uint64_t b, uint64_t e) {
+          float s = 0.f;
+          for (uint64_t i = b + lane; i < e; i += 32) {
+            const float d = a.delta[ldg(a.col + i)];
+            s += d > 0.f ? d : 0.f;
+          }
+          s = warp_sum(s);
+          if (lane == 0) atomicAdd(&a.acc[v], s);
+        });
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    for (uint64_t i = gtid; i < a.sched.nheavy; i += gthreads) {
+      const uint32_t v = a.sched.heavy_list[i];
+      const float sum = a.acc[v];
+      a.acc[v] = 0.f;
+      finish(v, sum);
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    const uint32_t accum = *reinterpret_cast<volatile uint32_t*>(&ctl->active[it % 3]);
+    if (gtid == 0) ctl->iters = it + 1;
+    if (it + 1 >= a.max_iter || accum == 0) break;
+  }
+}
+
+// ---- residual push, Sync (PageRank-push.cpp:103-188) ------------------------
+__global__ void pr_push_init(PrArgs a) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = tid; v < a.n; v += stride) {
+    a.value[v] = 0.f;
+    a.residual[v] = 1.0f - a.alpha;
+    a.active[0][v] = (uint32_t)v;
+    a.stamp[v] = 0xFFFFFFFFu;
+  }
+  if (tid == 0) a.ctl->active[0] = a.n;
+}
+
+__global__ void __launch_bounds__(kBlock) pr_push_persistent(PrArgs a) {
+  PrCtl* ctl = a.ctl;
+  const uint64_t deadline = kernel_deadline();
+  const uint64_t gtid = blockIdx.x * (uint64_t)kBlock + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * kBlock;
+  const uint32_t lane = lane_id();
+  unsigned long long my_push = 0;
+  for (uint32_t it = 0;; ++it) {
+    const uint32_t na = min(ctl->active[it % 3], a.n);
+    if (na == 0 || it >= a.max_iter) break;
+    const int fset = it % 3;
+    if (gtid == 0) {
+      ctl->active[(it + 2) % 3] = 0;
+      ctl->fc[(it + 1) % 3] = FrontierCounters{};
+    }
+    FrontierCounters& fc = ctl->fc[fset];
+    const uint32_t* act = a.active[it & 1];
+    uint32_t* act_next = a.active[(it + 1) & 1];
+    // phase A: absorb residual, compute delta, queue vertices with out-arcs
+    for (uint64_t base = gtid - lane; base < na; base += gthreads) {
+      const uint64_t i = base + lane;
+      bool q = false;
+      uint32_t v = 0;
+      if (i < na) {
+        v = act[i];
+        const float r = a.residual[v];
+        if (r > a.tol) {
+          const float old = atomicExch(&a.residual[v], 0.f);
+          if (old > 0.f) {
+            a.value[v] += old;
+            const uint64_t deg = ldg(a.offs + v + 1) - ldg(a.offs + v);
+            if (deg > 0) {
+              a.delta[v] = old * a.alpha / (float)deg;
+              q = true;
+            }
+          }
+        }
+      }
+      push_discovered(a.fq, it & 1, fc, q, v, a.offs, a.heavy, a.tile, &ctl->err);
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    // phase B: push deltas along out-arcs, activate on crossing tol
+    const uint32_t q_light = min(fc.light, a.fq.light_cap), q_tiles = min(fc.tiles, a.fq.tile_cap);
+    auto apply = [&](bool valid, uint32_t u, float d) {
+      bool act_u = false;
+      if (valid) {
+        const float old = atomicAdd(&a.residual[u], d);
+        ++my_push;
+        if (old <= a.tol && old + d >= a.tol) {
+          if (a.stamp[u] != it) act_u = atomicExch(&a.stamp[u], it) != it;
+        }
+      }
+      warp_push(act_u, u, act_next, &ctl->active[(it + 1) % 3], a.n, &ctl->err);
+    };
+    const uint32_t* qin = a.fq.light[it & 1];
+    const uint2* tin = a.fq.tiles[it & 1];
+    for (;;) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&fc.light_work, 32u);
+      base = __shfl_sync(kFull, base, 0);
+      if (base >= q_light) break;
+      const uint32_t idx = base + lane;
+      uint64_t b = 0;
+      uint32_t d = 0;
+      float dl = 0.f;
+      if (idx < q_light) {
+        const uint32_t v = qin[idx];
+        b = ldg(a.offs + v);
+        d = (uint32_t)(ldg(a.offs + v + 1) - b);
+        dl = a.delta[v];
+      }
+      warp_expand(b, d, __float_as_uint(dl), [&](bool valid, uint64_t e, uint32_t, uint32_t pl) {
+        apply(valid, valid ? ldg(a.col + e) : 0u, __uint_as_float(pl));
+      });
+    }
+    for (;;) {
+      uint32_t t = 0;
+      if (lane == 0) t = atomicAdd(&fc.tile_work, 1u);
+      t = __shfl_sync(kFull, t, 0);
+      if (t >= q_tiles) break;
+      const uint2 tv = tin[t];
+      const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
+      const uint64_t b = vb + (uint64_t)tv.y * a.tile;
+      const uint64_t e_end = min(ve, b + a.tile);
+      const float dl = a.delta[tv.x];
+      for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
+        const uint64_t e = e0 + lane;
+        apply(e < e_end, e < e_end ? ldg(a.col + e) : 0u, dl);
+      }
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    if (gtid == 0) ctl->iters = it + 1;
+  }
+  my_push = warp_sum(my_push);
+  if (lane == 0 && my_push) atomicAdd(&ctl->pushes, my_push);
+}
+
+int ensure_nout(gb_graph* g, cudaStream_t s) {
+  if (g->outdeg_of_stored) return GB_OK;
+  GB_CUDA(cudaMalloc(&g->outdeg_of_stored, sizeof(uint32_t) * g->n));
+  GB_CUDA(cudaMemsetAsync(g->outdeg_of_stored, 0, sizeof(uint32_t) * g->n, s));
+  if (g->m) count_nout<<<g->sm_count * 8, 256, 0, s>>>(g->col, g->m, g->outdeg_of_stored);
+  GB_CUDA(cudaGetLastError());
+  return GB_OK;
+}
+
+enum class PrKind { Pull, PullResidual, Push };
+
+inline float bits_to_float(uint32_t u) {
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
+int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_iter, float* rank_out,
+                 uint32_t* iters_out, gb_stats* stats, cudaStream_t s, float init = -1.f, float base = -1.f,
+                 int linf = 0) {
+  if (!(alpha > 0.f && alpha < 1.f)) GB_FAIL(GB_ERR_ARG, "pagerank: alpha must be in (0,1)");
+  if (!(tol >= 0.f)) GB_FAIL(GB_ERR_ARG, "pagerank: tolerance must be >= 0");
+  if (max_iter == 0) GB_FAIL(GB_ERR_ARG, "pagerank: max_iter must be > 0");
+  const gb_tuning t = effective_tuning(g);
+  const uint32_t n = g->n;
+  const bool out_dev = is_device_ptr(rank_out);
+  int st = GB_OK;
+  SweepSched sched{};
+  if (kind != PrKind::Push) {
+    st = ensure_sweep_schedule(g, t.heavy_degree, t.tile_edges, s, &sched);
+    if (st != GB_OK) return st;
+    st = ensure_nout(g, s);
+    if (st != GB_OK) return st;
+  }
+  FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
+  size_t need = carve_size<PrCtl>(1) + 4 * carve_size<float>(n) + (out_dev ? 0 : carve_size<float>(n));
+  if (kind != PrKind::Pull) need += 2 * carve_size<float>(n);
+  if (kind == PrKind::Push) need += 3 * carve_size<uint32_t>(n) + fl.bytes;
+  st = ws_reserve(g, need, s);
+  if (st != GB_OK) return st;
+  Carver cv(g->ws);
+  PrArgs a{};
+  a.ctl = cv.take<PrCtl>(1);
+  a.c[0] = cv.take<float>(n);
+  a.c[1] = cv.take<float>(n);
+  a.acc = cv.take<float>(n);
+  if (kind != PrKind::Pull) {
+    a.residual = cv.take<float>(n);
+    a.delta = cv.take<float>(n);
+  }
+  if (kind == PrKind::Push) {
+    a.active[0] = cv.take<uint32_t>(n);
+    a.active[1] = cv.take<uint32_t>(n);
+    a.stamp = cv.take<uint32_t>(n);
+    a.fq = carve_frontier(cv, fl);
+  }
+  a.value = out_dev ? rank_out : cv.take<float>(n);
+  a.offs = g->offs;
+  a.col = g->col;
+  a.nout = g->outdeg_of_stored;
+  a.n = n;
+  a.alpha = alpha;
+  a.base = base >= 0.f ? base : (1.0f - alpha) / (float)n;  // PageRank-pull.cpp:200
+  a.init = init >= 0.f ? init : 1.0f / (float)n;
+  a.linf = linf;
+  a.tol = tol;
+  a.max_iter = max_iter;
+  a.sched = sched;
+  a.heavy = t.heavy_degree;
+  a.tile = t.tile_edges;
+  GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(PrCtl), s));
+  const void* kfn = nullptr;
+  if (kind == PrKind::Pull) {
+    pr_pull_init<<<g->sm_count * 4, 256, 0, s>>>(a);
+    kfn = reinterpret_cast<const void*>(&pr_pull_persistent);
+  } else if (kind == PrKind::PullResidual) {
+    pr_resid_init<<<g->sm_count * 4, 256, 0, s>>>(a);
+    GB_CUDA(cudaMemsetAsync(a.acc, 0, sizeof(float) * n, s));
+    kfn = reinterpret_cast<const void*>(&pr_pull_residual_persistent);
+  } else {
+    pr_push_init<<<g->sm_count * 4, 256, 0, s>>>(a);
+    kfn = reinterpret_cast<const void*>(&pr_push_persistent);
+  }
+  GB_CUDA(cudaGetLastError());
+  const int grid = coop_grid(g, kfn, kBlock, 0, t.blocks_per_sm);
+  if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "pagerank: cannot size cooperative grid");
+  void* args[] = {&a};
+  GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, kBlock, args, 0, s));
+  PrCtl* hc = reinterpret_cast<PrCtl*>(static_cast<char*>(g->pinned) + 256);
+  GB_CUDA(cudaMemcpyAsync(hc, a.ctl, sizeof(PrCtl), cudaMemcpyDeviceToHost, s));
+  if (!out_dev) {
+    st = copy_out(rank_out, a.value, sizeof(float) * n, s);
+    if (st != GB_OK) return st;
+  }
+  if (stats || iters_out || !out_dev) {
+    GB_CUDA(cudaStreamSynchronize(s));
+    if (hc->err) return dev_err_status(hc->err, "pagerank");
+    if (iters_out) *iters_out = hc->iters;
+    if (stats) {
+      *stats = gb_stats{};
+      stats->vertices_reached = n;
+      stats->edges_reached = g->m;
+      stats->rounds = hc->iters;
+      stats->relaxations = hc->pushes;
+      stats->launches = 2;
+      stats->residual = kind == PrKind::Pull ? (linf ? (double)bits_to_float(hc->linf[(hc->iters + 2) % 3])
+                                                     : hc->l1[(hc->iters + 2) % 3])
+                                             : 0.0;
+    }
+    if (kind != PrKind::Push && hc->iters >= max_iter) {
+      // the ranks are set; the status tells the caller the cap was hit
+      gb::set_error("pagerank: failed to converge in %u iterations", hc->iters);
+      return GB_ERR_NOT_CONVERGED;
+    }
+  }
+  return GB_OK;
+}
+
+}  // namespace
+
+}  // namespace gb
+
+extern "C" {
+
+int gb_pagerank_pull(gb_graph* g, float alpha, float tol, uint32_t max_iter, float* rank_out,
+                     uint32_t* iters_out, gb_stats* stats, void* stream) {
+  gb::clear_error();
+  if (!g || !rank_out) GB_FAIL(GB_ERR_ARG, "gb_pagerank_pull: null argument");
+  GB_CUDA(cudaSetDevice(g->device));
+  return gb::run_pagerank(g, gb::PrKind::Pull, alpha, tol, max_iter, rank_out, iters_out, stats,
+                          static_cast<cudaStream_t>(stream));
+}
+
+int gb_pagerank_pull_ex(gb_graph* g, float alpha, float tol, uint32_t max_iter, float init, float base,
+                        int norm_linf, float* rank_out, uint32_t* iters_out, gb_stats* stats, void* stream) {
+  gb::clear_error();
+  if (!g || !rank_out) GB_FAIL(GB_ERR_ARG, "gb_pagerank_pull_ex: null argument");
+  if (!(init >= 0.f) || !(base >= 0.f)) GB_FAIL(GB_ERR_ARG, "gb_pagerank_pull_ex: init and base must be >= 0");
+  GB_CUDA(cudaSetDevice(g->device));
+  return gb::run_pagerank(g, gb::PrKind::Pull, alpha, tol, max_iter, rank_out, iters_out, stats,
+                          static_cast<cudaStream_t>(stream), init, base, norm_linf ? 1 : 0);
+}
+
+int gb_pagerank_pull_residual(gb_graph* g, float alpha, float tol, uint32_t max_iter, float* rank_out,
+                              uint32_t* iters_out, gb_stats* stats, void* stream) {
+  gb::clear_error();
+  if (!g || !rank_out) GB_FAIL(GB_ERR_ARG, "gb_pagerank_pull_residual: null argument");
+  GB_CUDA(cudaSetDevice(g->device));
+  return gb::run_pagerank(g, gb::PrKind::PullResidual, alpha, tol, max_iter, rank_out, iters_out, stats,
+                          static_cast<cudaStream_t>(stream));
+}
+
+int gb_pagerank_push(gb_graph* g, float alpha, float tol, uint32_t max_iter, float* rank_out,
+                     uint32_t* iters_out, gb_stats* stats, void* stream) {
+  gb::clear_error();
+  if (!g || !rank_out) GB_FAIL(GB_ERR_ARG, "gb_pagerank_push: null argument");
+  GB_CUDA(cudaSetDevice(g->device));
+  return gb::run_pagerank(g, gb::PrKind::Push, alpha, tol, max_iter, rank_out, iters_out, stats,
+                          static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

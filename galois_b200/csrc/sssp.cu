@@ -1,0 +1,346 @@
+// Delta-stepping single-source shortest paths over uint32 arc weights.
+//
+// Reference semantics: lonestar/analytics/cpu/sssp/SSSP.cpp:118-173
+// (deltaStepAlgo: OBIM buckets indexed by dist >> stepShift, relax with
+// atomicMin(dist[dst], dist[src]+w), push on improvement), default shift 13
+// (SSSP.cpp:53-56).  Shortest distances are unique, so the output is
+// bit-identical to the CPU app for any schedule.
+//
+// B200 design: one cooperative persistent launch.  OBIM becomes
+//   * a near queue (light vertices + heavy-vertex edge tiles, frontier.cuh)
+//     holding vertices whose tentative distance lies in the current bucket;
+//     duplicate pushes within a phase are filtered by a per-vertex phase stamp;
+//   * a far pile holding vertices relaxed beyond the bucket (membership
+//     bitmap, so each vertex is in the pile at most once).
+// A phase relaxes every near vertex with its CURRENT distance (no stale
+// items); when the near queue drains, the far pile is split: settled entries
+// are dropped, the minimum remaining bucket becomes current (empty buckets
+// are skipped), its vertices move to the near queue and the rest are
+// compacted.  Phases are separated by a bounded grid barrier.
+
+#include "device_common.cuh"
+#include "device_graph.cuh"
+#include "frontier.cuh"
+
+namespace gb {
+
+namespace {
+
+struct SsspCtl {
+  GridBar bar;
+  int err;
+  uint32_t pad0;
+  FrontierCounters fc[3];
+  uint32_t far_count[2];
+  uint32_t min_bucket;
+  uint32_t buckets;
+  uint32_t phases;
+  uint32_t pad1;
+  unsigned long long scanned;
+  unsigned long long relax;
+};
+
+struct SsspArgs {
+  const uint64_t* __restrict__ offs;
+  const uint32_t* __restrict__ col;
+  const uint32_t* __restrict__ w;
+  uint32_t n;
+  uint32_t src;
+  uint32_t shift;
+  uint32_t* dist;
+  uint32_t* stamp;  // phase in which the vertex was last queued (near)
+  uint32_t* infar;  // bitmap: vertex currently in the far pile
+  uint32_t* far[2];
+  FrontierQueues fq;
+  SsspCtl* ctl;
+  uint32_t heavy;
+  uint32_t tile;
+  uint32_t max_phases;
+};
+
+__global__ void sssp_init(SsspArgs a) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t words = (a.n + 31) >> 5;
+  for (uint64_t v = tid; v < a.n; v += stride) {
+    a.dist[v] = (v == a.src) ? 0u : kInf;
+    a.stamp[v] = (v == a.src) ? 0u : 0xFFFFFFFFu;
+  }
+  for (uint64_t w = tid; w < words; w += stride) a.infar[w] = 0;
+  if (tid == 0) {
+    const uint64_t d = a.offs[a.src + 1] - a.offs[a.src];
+    FrontierCounters& c = a.ctl->fc[0];
+    c.vertices = 1;
+    c.degree_sum = d;
+    if (d > 0) seed_vertex(a.fq, 0, c, a.src, d, a.heavy, a.tile);
+  }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
+  SsspCtl* ctl = a.ctl;
+  const unsigned nblocks = gridDim.x;
+  const uint64_t deadline = kernel_deadline();
+  const uint32_t lane = lane_id();
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  unsigned long long my_scanned = 0, my_relax = 0;
+
+  uint32_t bucket = 0;  // current bucket index; near items have dist < hi
+  int fp = 0;           // far pile being appended to
+  uint32_t P = 0;       // phase counter (counter set P%3, queue buffer P&1)
+
+  for (;;) {
+    if (P >= a.max_phases) {
+      if (gtid == 0) raise_err(&ctl->err, kDevMaxRounds);
+      break;
+    }
+    const int rd = P % 3, wr = (P + 1) % 3, cl = (P + 2) % 3;
+    FrontierCounters& cur = ctl->fc[rd];
+    FrontierCounters& nxt = ctl->fc[wr];
+    const uint32_t q_light = min(cur.light, a.fq.light_cap), q_tiles = min(cur.tiles, a.fq.tile_cap);
+    if (gtid == 0) {
+      ctl->fc[cl] = FrontierCounters{};
+      ctl->far_count[fp ^ 1] = 0;  // previous pile is dead once split
+    }
+    const uint32_t next_stamp = P + 1;
+    const uint64_t hi64 = ((uint64_t)bucket + 1) << a.shift;
+    const uint32_t hi = hi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)hi64;
+    uint32_t* farq = a.far[fp];
+
+    // relax one arc; all lanes call (warp collectives inside)
+    auto relax = [&](bool valid, uint32_t u, uint32_t nd) {
+      bool to_near = false, to_far = false;
+      if (valid && nd < a.dist[u]) {
+        const uint32_t old = atomicMin(&a.dist[u], nd);
+        if (nd < old) {
+          ++my_relax;
+          if (nd < hi) {
+            if (a.stamp[u] != next_stamp) to_near = atomicExch(&a.stamp[u], next_stamp) != next_stamp;
+          } else {
+            const uint32_t bit = 1u << (u & 31);
+            if (!(a.infar[u >> 5] & bit)) to_far = !(atomicOr(&a.infar[u >> 5], bit) & bit);
+          }
+        }
+      }
+      push_discovered(a.fq, (P + 1) & 1, nxt, to_near, u, a.offs, a.heavy, a.tile, &ctl->err);
+      warp_push(to_far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
+    };
+
+    if (q_light != 0 || q_tiles != 0) {
+      // ---- relaxation phase --------------------------------------------
+      const uint32_t* qin = a.fq.light[P & 1];
+      const uint2* tin = a.fq.tiles[P & 1];
+      for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&cur.light_work, 32u);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= q_light) break;
+        const uint32_t idx = base + lane;
+        uint64_t b = 0;
+        uint32_t d = 0, dv = 0;
+        if (idx < q_light) {
+          const uint32_t v = qin[idx];
+          b = ldg(a.offs + v);
+          d = (uint32_t)(ldg(a.offs + v + 1) - b);
+          dv = a.dist[v];
+        }
+        my_scanned += d;
+        warp_expand(b, d, dv, [&](bool valid, uint64_t e, uint32_t, uint32_t dsrc) {
+          uint32_t u = 0, nd = 0;
+          if (valid) {
+            u = ldg(a.col + e);
+            nd = dsrc + ldg(a.w + e);
+          }
+          relax(valid, u, nd);
+        });
+      }
+      for (;;) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(&cur.tile_work, 1u);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= q_tiles) break;
+        const uint2 tv = tin[t];
+        const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
+        const uint64_t b = vb + (uint64_t)tv.y * a.tile;
+        const uint64_t e_end = min(ve, b + a.tile);
+        const uint32_t dsrc = a.dist[tv.x];
+        if (lane == 0) my_scanned += e_end - b;
+        for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
+          const uint64_t e = e0 + lane;
+          const bool valid = e < e_end;
+          uint32_t u = 0, nd = 0;
+          if (valid) {
+            u = ldg(a.col + e);
+            nd = dsrc + ldg(a.w + e);
+          }
+          relax(valid, u, nd);
+        }
+      }
+      if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+      ++P;
+      continue;
+    }
+
+    // ---- near queue drained: advance to the next non-empty bucket --------
+    const uint32_t nfar = min(ctl->far_count[fp], a.n);
+    if (nfar == 0) break;  // nothing left anywhere
+    if (gtid == 0) {
+      ctl->min_bucket = 0xFFFFFFFFu;
+      ctl->buckets += 1;
+    }
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    // R1: minimum bucket among far entries not yet settled
+    {
+      uint32_t mb = 0xFFFFFFFFu;
+      for (uint64_t i = gtid; i < nfar; i += gthreads) {
+        const uint32_t d = a.dist[farq[i]];
+        if (d >= hi) mb = min(mb, d >> a.shift);
+      }
+      mb = __reduce_min_sync(kFull, mb);
+      if (lane == 0 && mb != 0xFFFFFFFFu) atomicMin(&ctl->min_bucket, mb);
+    }
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    const uint32_t nb = ctl->min_bucket;
+    if (nb == 0xFFFFFFFFu) break;  // every far entry was settled
+    // R2: split the pile into the near queue (bucket nb) and the other pile
+    {
+      const uint64_t nhi64 = ((uint64_t)nb + 1) << a.shift;
+      const uint32_t nhi = nhi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)nhi64;
+      uint32_t* keepq = a.far[fp ^ 1];
+      for (uint64_t base = gtid - lane; base < nfar; base += gthreads) {
+        const uint64_t i = base + lane;
+        bool to_near = false, keep = false;
+        uint32_t u = 0;
+        if (i < nfar) {
+          u = farq[i];
+          const uint32_t d = a.dist[u];
+          if (d >= hi && d < nhi) {
+            to_near = true;
+            a.stamp[u] = next_stamp;
+          } else if (d >= nhi) {
+            keep = true;
+          }
+          if (!keep) atomicAnd(&a.infar[u >> 5], ~(1u << (u & 31)));
+        }
+        push_discovered(a.fq, (P + 1) & 1, nxt, to_near, u, a.offs, a.heavy, a.tile, &ctl->err);
+        warp_push(keep, u, keepq, &ctl->far_count[fp ^ 1], a.n, &ctl->err);
+      }
+    }
+    bucket = nb;
+    fp ^= 1;
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    ++P;
+  }
+  my_scanned = warp_sum(my_scanned);
+  my_relax = warp_sum(my_relax);
+  if (lane == 0) {
+    if (my_scanned) atomicAdd(&ctl->scanned, my_scanned);
+    if (my_relax) atomicAdd(&ctl->relax, my_relax);
+  }
+  if (gtid == 0) ctl->phases = P;
+}
+
+__global__ void sssp_reach_kernel(const uint32_t* __restrict__ dist, const uint64_t* __restrict__ offs,
+                                  uint32_t n, unsigned long long* out) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long nr = 0, mr = 0;
+  for (uint64_t v = tid; v < n; v += stride) {
+    if (dist[v] != kInf) {
+      nr += 1;
+      mr += offs[v + 1] - offs[v];
+    }
+  }
+  nr = warp_sum(nr);
+  mr = warp_sum(mr);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(out, nr);
+    atomicAdd(out + 1, mr);
+  }
+}
+
+}  // namespace
+
+int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_stats* stats,
+             cudaStream_t s) {
+  if (!g->w) GB_FAIL(GB_ERR_ARG, "gb_sssp_delta: graph has no uint32 edge weights");
+  if (shift > 31) GB_FAIL(GB_ERR_ARG, "gb_sssp_delta: delta shift %u > 31", shift);
+  const gb_tuning t = effective_tuning(g);
+  const uint32_t n = g->n;
+  const uint32_t words = (n + 31) / 32;
+  const bool out_dev = is_device_ptr(dist_out);
+  FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
+  const size_t need = carve_size<SsspCtl>(1) + carve_size<uint32_t>(n) + carve_size<uint32_t>(words) +
+                      2 * carve_size<uint32_t>(n) + fl.bytes + (out_dev ? 0 : carve_size<uint32_t>(n)) +
+                      carve_size<unsigned long long>(2);
+  int st = ws_reserve(g, need, s);
+  if (st != GB_OK) return st;
+  Carver cv(g->ws);
+  SsspArgs a{};
+  a.ctl = cv.take<SsspCtl>(1);
+  a.stamp = cv.take<uint32_t>(n);
+  a.infar = cv.take<uint32_t>(words);
+  a.far[0] = cv.take<uint32_t>(n);
+  a.far[1] = cv.take<uint32_t>(n);
+  a.fq = carve_frontier(cv, fl);
+  unsigned long long* reach = cv.take<unsigned long long>(2);
+  a.dist = out_dev ? dist_out : cv.take<uint32_t>(n);
+  a.offs = g->offs;
+  a.col = g->col;
+  a.w = g->w;
+  a.n = n;
+  a.src = src;
+  a.shift = shift;
+  a.heavy = t.heavy_degree;
+  a.tile = t.tile_edges;
+  a.max_phases = 0x7FFFFFFFu;
+  GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), s));
+  sssp_init<<<g->sm_count * 4, 256, 0, s>>>(a);
+  GB_CUDA(cudaGetLastError());
+  const void* kfn = reinterpret_cast<const void*>(&sssp_persistent<256>);
+  const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
+  if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
+  void* args[] = {&a};
+  GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, args, 0, s));
+  int* pin = static_cast<int*>(g->pinned);
+  GB_CUDA(cudaMemcpyAsync(pin, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (stats) {
+    GB_CUDA(cudaMemsetAsync(reach, 0, 16, s));
+    sssp_reach_kernel<<<g->sm_count * 4, 256, 0, s>>>(a.dist, g->offs, n, reach);
+    SsspCtl* hc = reinterpret_cast<SsspCtl*>(static_cast<char*>(g->pinned) + 256);
+    unsigned long long* hr = reinterpret_cast<unsigned long long*>(static_cast<char*>(g->pinned) + 2048);
+    GB_CUDA(cudaMemcpyAsync(hc, a.ctl, sizeof(SsspCtl), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(hr, reach, 16, cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    stats->vertices_reached = hr[0];
+    stats->edges_reached = hr[1];
+    stats->edges_scanned = hc->scanned;
+    stats->relaxations = hc->relax;
+    stats->rounds = hc->phases;
+    stats->pull_rounds = 0;
+    stats->buckets = hc->buckets + 1;
+    stats->launches = 3;
+    stats->residual = 0;
+  }
+  if (!out_dev) {
+    st = copy_out(dist_out, a.dist, sizeof(uint32_t) * n, s);
+    if (st != GB_OK) return st;
+  }
+  if (stats || !out_dev) {
+    GB_CUDA(cudaStreamSynchronize(s));
+    if (*pin) return dev_err_status(*pin, "gb_sssp_delta");
+  }
+  return GB_OK;
+}
+
+}  // namespace gb
+
+extern "C" int gb_sssp_delta(gb_graph* g, uint32_t src, uint32_t delta_shift, uint32_t* dist_out,
+                             gb_stats* stats, void* stream) {
+  gb::clear_error();
+  if (!g || !dist_out) GB_FAIL(GB_ERR_ARG, "gb_sssp_delta: null argument");
+  if (src >= g->n) GB_FAIL(GB_ERR_ARG, "gb_sssp_delta: source %u >= n %u", src, g->n);
+  GB_CUDA(cudaSetDevice(g->device));
+  return gb::run_sssp(g, src, delta_shift, dist_out, stats, static_cast<cudaStream_t>(stream));
+}

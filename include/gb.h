@@ -1,0 +1,275 @@
+/*
+ * gb.h -- C ABI of the B200-native CSR edge-map library (libgb.so).
+ *
+ * This header is the drop-in boundary for the Galois lonestar analytics hot
+ * path: BFS, delta-stepping SSSP, label-propagation connected components,
+ * PageRank (pull-topological and residual-push), Brandes betweenness
+ * centrality, and a differentiable personalised PageRank.  Every entry point
+ * takes plain pointers and sizes, returns an int status (GB_OK == 0, negative
+ * on error, message in gb_last_error()), and never aborts or exits.
+ *
+ * Reference interfaces replaced (paths relative to the Galois source tree):
+ *   graph + .gr I/O     libgalois/include/galois/graphs/LC_CSR_Graph.h:879-1011
+ *                       (readGraphFromGRFile), libgalois/src/FileGraph.cpp:44-53
+ *                       (format), libgpu/src/csr_graph.cu:172-315 (device mirror)
+ *   per-operator C ABI  lonestar/analytics/distributed/bfs/bfs_push_cuda.h:103-145
+ *                       (BFS_cuda / InitializeGraph_allNodes_cuda pattern over
+ *                       an opaque struct CUDA_Context*)
+ *   algorithms          lonestar/analytics/cpu/bfs/bfs.cpp:244-293,
+ *                       lonestar/analytics/cpu/sssp/SSSP.cpp:118-173,
+ *                       lonestar/analytics/cpu/connected-components/
+ *                       ConnectedComponents.cpp:183-230,
+ *                       lonestar/analytics/cpu/pagerank/PageRank-pull.cpp:196-251,
+ *                       lonestar/analytics/cpu/pagerank/PageRank-push.cpp:68-188,
+ *                       lonestar/analytics/cpu/betweennesscentrality/
+ *                       LevelStructs.h:87-185
+ *   python entry points python/galois/_bfs.pyx:171, _sssp.pyx:154,
+ *                       _pagerank.pyx:157, _connected_components.pyx:87
+ *
+ * Conventions
+ *   - Node ids are uint32; edge offsets are uint64.  Offsets passed IN follow
+ *     the LC_CSR_Graph layout: n END offsets, begin(v) = v ? end[v-1] : 0
+ *     (LC_CSR_Graph.h:142,172-178).
+ *   - Unreached BFS/SSSP vertices hold GB_DIST_INFINITY = UINT_MAX/2-1
+ *     (lonestar/liblonestar/include/Lonestar/BFS_SSSP.h:31-32).
+ *   - Output buffers may be host or device memory; the library detects which.
+ *     Device outputs keep the call asynchronous on `stream` (unless `stats` is
+ *     non-NULL, which synchronises the stream to read counters).
+ *   - `stream` is a cudaStream_t passed as void*; NULL means the legacy
+ *     default stream.
+ *   - A gb_graph handle is not re-entrant: use one handle per host thread.
+ */
+#ifndef GB_H
+#define GB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GB_OK 0
+#define GB_ERR_ARG (-1)           /* bad argument (null pointer, id >= n, ...) */
+#define GB_ERR_OOM (-2)           /* host or device allocation failed          */
+#define GB_ERR_CUDA (-3)          /* a CUDA runtime call failed                */
+#define GB_ERR_TIMEOUT (-4)       /* a bounded device wait or loop gave up     */
+#define GB_ERR_FILE (-5)          /* file could not be opened/read/written     */
+#define GB_ERR_FORMAT (-6)        /* malformed .gr / edge list                 */
+#define GB_ERR_NOT_CONVERGED (-7) /* iteration cap reached (result still set)  */
+#define GB_ERR_UNSUPPORTED (-8)   /* valid request this build does not handle  */
+#define GB_ERR_CAPACITY (-9)      /* input larger than a fixed-size buffer     */
+
+#define GB_DIST_INFINITY 2147483646u /* std::numeric_limits<uint32_t>::max()/2-1 */
+
+/* Last error message of the calling host thread ("" if none). */
+const char* gb_last_error(void);
+/* Library version: major*10000 + minor*100 + patch. */
+int gb_version(void);
+
+/* ---- host-side CSR (no GPU needed) -------------------------------------- */
+/* Arrays are malloc'd by the library and released by gb_host_csr_free.
+ * end_offs follows the LC_CSR_Graph end-offset layout (n entries). */
+typedef struct gb_host_csr {
+  uint32_t n;
+  uint64_t m;
+  uint64_t* end_offs; /* [n]                         */
+  uint32_t* col;      /* [m] destination ids         */
+  uint32_t* w_u32;    /* [m] or NULL (integer weights) */
+  float* w_f32;       /* [m] or NULL (float weights)   */
+} gb_host_csr;
+
+void gb_host_csr_init(gb_host_csr* g);
+void gb_host_csr_free(gb_host_csr* g);
+
+/* .gr v1/v2 reader (FileGraph.cpp:44-53, 104-135; LC_CSR_Graph.h:879-1011).
+ * edge_bytes selects how the edge-data section is interpreted:
+ *   0 = ignore, 4 = uint32 weights into w_u32, -4 = float weights into w_f32.
+ * A file whose sizeofEdge differs from |edge_bytes| (when non-zero) is
+ * rejected with GB_ERR_FORMAT. */
+int gb_gr_read(const char* path, int edge_bytes, gb_host_csr* out);
+/* .gr v1 writer: edge_bytes 0 (void), 4 (w_u32) or -4 (w_f32). */
+int gb_gr_write(const char* path, const gb_host_csr* g, int edge_bytes);
+/* Text edge lists (tools/graph-convert/graph-convert.cpp:351-530):
+ * "src dst" per line, or "src<delim>dst" with skip_first_line for CSV.
+ * Lines that do not parse are ignored; per-source order is preserved. */
+int gb_edgelist_to_csr(const char* path, int skip_first_line, char delim,
+                       gb_host_csr* out);
+/* gr2edgelist (graph-convert.cpp:867-900): "src dst\n" per edge. */
+int gb_csr_to_edgelist(const char* path, const gb_host_csr* g);
+
+/* Seeded synthetic generators (SplitMix64 counter-based streams).
+ * RMAT: edge_factor * 2^scale draws with quadrant probabilities a,b,c
+ * (d = 1-a-b-c); self-loops and duplicate arcs removed; if symmetrize, every
+ * arc gets its reverse; if permute, vertex ids are relabelled by a seeded
+ * random permutation (perm_out[i] = new id of generator vertex i, may be
+ * NULL).  Adjacency lists are sorted ascending. */
+int gb_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b,
+                double c, uint64_t seed, int symmetrize, int permute,
+                uint32_t* perm_out, gb_host_csr* out);
+/* rows x cols 4-neighbour grid, both arc directions, row-major ids. */
+int gb_gen_grid2d(uint32_t rows, uint32_t cols, gb_host_csr* out);
+/* Erdos-Renyi G(n, M) with M = round(n*mean_degree/2) undirected draws,
+ * symmetrised, self-loops and duplicates removed. */
+int gb_gen_er(uint32_t n, double mean_degree, uint64_t seed, gb_host_csr* out);
+/* Per-arc weights by CSR position: uint32 uniform in [lo,hi], or float
+ * uniform in (0,1]. */
+int gb_assign_weights_u32(gb_host_csr* g, uint32_t lo, uint32_t hi,
+                          uint64_t seed);
+int gb_assign_weights_f32(gb_host_csr* g, uint64_t seed);
+/* Transpose (LC_CSR_Graph.h:617-712 semantics): arcs u->v become v->u, edge
+ * data follows its arc, adjacency sorted by source id.  If edge_map is
+ * non-NULL it receives, for every transposed arc, its index in g. */
+int gb_transpose_host(const gb_host_csr* g, gb_host_csr* out,
+                      uint64_t* edge_map);
+
+/* ---- device graph ------------------------------------------------------- */
+typedef struct gb_graph gb_graph;
+
+/* Upload a CSR to `device`.  end_offs: LC layout (n entries).  Either weight
+ * array may be NULL.  symmetric != 0 declares in-edges == out-edges (the
+ * -symmetricGraph flag, BoilerPlate.cpp:38-41), which enables pull/bottom-up
+ * steps without a transpose.  Inputs may be host or device pointers. */
+int gb_graph_upload(const uint64_t* end_offs, const uint32_t* col,
+                    const uint32_t* w_u32, const float* w_f32, uint32_t n,
+                    uint64_t m, int symmetric, int device, gb_graph** out);
+int gb_graph_load_gr(const char* path, int edge_bytes, int symmetric,
+                     int device, gb_graph** out);
+int gb_graph_free(gb_graph* g);
+int gb_graph_info(const gb_graph* g, uint32_t* n, uint64_t* m,
+                  int* symmetric);
+/* Device-resident begin offsets (n+1), columns and weights (NULL if absent):
+ * lets a caller build operators (include/gb_operator.cuh) over the mirror. */
+int gb_graph_device_arrays(const gb_graph* g, const uint64_t** offs,
+                           const uint32_t** col, const uint32_t** w_u32,
+                           const float** w_f32);
+/* Build the in-edge (transposed) CSR on the device, with the map from each
+ * transposed arc to its original arc.  Needed for pull/bottom-up steps on
+ * directed graphs and for the PPR forward pass. */
+int gb_graph_build_transpose(gb_graph* g, void* stream);
+
+/* Per-call statistics (all optional). */
+typedef struct gb_stats {
+  uint64_t vertices_reached; /* n_r                                          */
+  uint64_t edges_reached;    /* m_r = sum of out-degrees of reached vertices  */
+  uint64_t edges_scanned;    /* arcs actually read                           */
+  uint64_t relaxations;      /* successful atomicMin / pushes                */
+  uint32_t rounds;           /* levels / phases / sweeps / iterations        */
+  uint32_t pull_rounds;      /* bottom-up rounds (BFS)                       */
+  uint32_t buckets;          /* delta buckets processed (SSSP)               */
+  uint32_t launches;         /* kernels launched by this call                */
+  double residual;           /* final L1 residual (PageRank)                 */
+} gb_stats;
+
+/* Tuning knobs; zero fields mean "library default / autotuned". */
+typedef struct gb_tuning {
+  uint32_t heavy_degree; /* vertices above this degree are edge-tiled      */
+  uint32_t tile_edges;   /* edges per tile for heavy vertices              */
+  uint32_t block_threads;/* CTA size for persistent kernels (multiple of 32)*/
+  uint32_t blocks_per_sm;/* persistent CTAs per SM (0 = max resident)      */
+  float do_alpha;        /* push->pull switch (bfsDirectionOpt.cpp:68-72)  */
+  float do_beta;         /* pull->push switch (bfsDirectionOpt.cpp:73-77)  */
+  int direction_opt;     /* 0 = pull steps allowed when in-edges exist, 2 = push only */
+} gb_tuning;
+int gb_graph_set_tuning(gb_graph* g, const gb_tuning* t);
+int gb_graph_get_tuning(const gb_graph* g, gb_tuning* t);
+
+/* BFS levels from src (bfs.cpp:244-293; bfsDirectionOpt.cpp:204-342 for
+ * the push/pull switch).  level_out[n], unreached = GB_DIST_INFINITY. */
+int gb_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats,
+           void* stream);
+
+/* Delta-stepping SSSP over uint32 weights (SSSP.cpp:118-173, -delta is a
+ * shift: bucket = dist >> delta_shift).  dist_out[n]. */
+int gb_sssp_delta(gb_graph* g, uint32_t src, uint32_t delta_shift,
+                  uint32_t* dist_out, gb_stats* stats, void* stream);
+
+/* Connected components of a symmetric graph; label = minimum vertex id of the
+ * component, as LabelProp converges to (ConnectedComponents.cpp:183-230).
+ * algo: 0 = label propagation with pointer jumping, 1 = union-find hooking
+ * (one sweep), 2 = Afforest-style sampling then hooking. */
+#define GB_CC_LABELPROP 0
+#define GB_CC_UNIONFIND 1
+#define GB_CC_AFFOREST 2
+int gb_cc(gb_graph* g, int algo, uint32_t* label_out, gb_stats* stats,
+          void* stream);
+
+/* PageRank pull-topological over the graph as stored, which must be the
+ * TRANSPOSE of the web graph (the -transposedGraph contract,
+ * PageRank-pull.cpp:196-251): rank = alpha*sum(rank[u]/nout[u]) +
+ * (1-alpha)/n, nout counted from the stored graph, stop when the L1 change
+ * <= tol or after max_iter iterations.  rank_out[n] float. */
+int gb_pagerank_pull(gb_graph* g, float alpha, float tol, uint32_t max_iter,
+                     float* rank_out, uint32_t* iters_out, gb_stats* stats,
+                     void* stream);
+/* The pull-topological kernel with the initial rank, the base score and the
+ * stopping norm as parameters.  python/galois/_pagerank.pyx:86-139 uses
+ * init = base = 1-alpha and stops on the MAX |delta| (norm_linf = 1);
+ * gb_pagerank_pull is init = 1/n, base = (1-alpha)/n, L1 norm. */
+int gb_pagerank_pull_ex(gb_graph* g, float alpha, float tol, uint32_t max_iter,
+                        float init, float base, int norm_linf,
+                        float* rank_out, uint32_t* iters_out, gb_stats* stats,
+                        void* stream);
+/* PageRank residual push over out-edges (PageRank-push.cpp:103-188, Sync):
+ * value starts 0, residual 1-alpha; a vertex whose residual exceeds tol
+ * absorbs it and pushes residual*alpha/outdeg to its out-neighbours. */
+int gb_pagerank_push(gb_graph* g, float alpha, float tol, uint32_t max_iter,
+                     float* rank_out, uint32_t* iters_out, gb_stats* stats,
+                     void* stream);
+/* PageRank pull-residual (PageRank-pull.cpp:132-190): delta/residual rounds
+ * over the stored (transposed) graph. */
+int gb_pagerank_pull_residual(gb_graph* g, float alpha, float tol,
+                              uint32_t max_iter, float* rank_out,
+                              uint32_t* iters_out, gb_stats* stats,
+                              void* stream);
+
+/* Brandes betweenness centrality (LevelStructs.h:87-185) accumulated over
+ * srcs[0..nsrc).  batch = sources per multi-source launch (1..64); batch 1
+ * runs the single-source level-synchronous kernels once per source.
+ * fp64 path counts, fp32 dependencies; bc_out[n] float. */
+int gb_bc(gb_graph* g, const uint32_t* srcs, uint32_t nsrc, uint32_t batch,
+          float* bc_out, gb_stats* stats, void* stream);
+
+/* Many disjoint graphs in one launch: the graphs are packed block-diagonally
+ * into `g` (vertex ranges graph_first[k] .. graph_first[k+1]-1, k < ngraphs),
+ * BFS runs from graph_first[k] + local_src[k] for every k at once and CC
+ * labels every graph.  Labels are local ids (min local id of the component),
+ * levels are per-graph BFS levels.  level_out/label_out: [n]. */
+int gb_multi_graph_bfs_cc(gb_graph* g, const uint32_t* graph_first,
+                          uint32_t ngraphs, const uint32_t* local_src,
+                          uint32_t* level_out, uint32_t* label_out,
+                          gb_stats* stats, void* stream);
+
+/* Personalised PageRank, batched over B teleport vectors, on a directed graph
+ * with positive float edge weights w (arc j->i).  W~ = w / colsum (column-
+ * normalised by source out-weight).  Solves x = (1-alpha) T + alpha W~ x by
+ * Jacobi iteration to max-column L1 change <= tol.
+ *   teleport: dense [n][B] row-major float (device or host)
+ *   x_out:    [n][B] row-major float
+ * The graph needs gb_graph_build_transpose (done on first use). */
+int gb_ppr_forward(gb_graph* g, uint32_t B, const float* teleport, float alpha,
+                   float tol, uint32_t max_iter, float* x_out,
+                   uint32_t* iters_out, gb_stats* stats, void* stream);
+/* Adjoint of gb_ppr_forward: given x (forward solution) and gx = dL/dx, solves
+ * (I - alpha W~)^T lam = gx and returns
+ *   grad_teleport[n][B] = (1-alpha) lam
+ *   grad_w[m]           = dL/dw for every arc (summed over the batch),
+ *                         through the column normalisation.
+ * Either output may be NULL. */
+int gb_ppr_backward(gb_graph* g, uint32_t B, const float* x, const float* gx,
+                    float alpha, float tol, uint32_t max_iter,
+                    float* grad_teleport, float* grad_w, uint32_t* iters_out,
+                    gb_stats* stats, void* stream);
+
+/* Autotuner: times candidate degree-bin thresholds, tile sizes, CTA shapes
+ * and push/pull switch points for `kernel` ("bfs", "sssp", "cc", "pr") on this
+ * graph, keeps the fastest in the handle, and (if cache_path is non-NULL)
+ * merges it into a JSON-lines cache keyed by graph class and kernel. */
+int gb_autotune(gb_graph* g, const char* kernel, uint32_t src,
+                const char* cache_path, gb_tuning* best_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GB_H */

@@ -1,0 +1,214 @@
+"""ORACLE -- test infrastructure only.
+
+ctypes wrapper of oracle/liboracle.so, the CPU (C++17/OpenMP) restatement of
+the Galois lonestar algorithms on the CSR edge-map path (see oracle.cpp for the
+reference lines each function follows and how the restatement is pinned).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+arm may import this package; the product never does.
+
+Parity status: the reference cannot be built or run here (Boost, LLVM
+CommandLine and fmt are absent; the GPU apps need the un-vendored moderngpu
+submodule) and ships no golden outputs for this path, so there are no
+reference-run outputs.  The restatement is pinned by the reference's own
+verifiers (restated and run on every output), the graph-convert fixtures
+(tools/graph-convert/test-inputs) for the .gr path, and closed-form known
+answers.  PageRank and BC beyond closed-form cases are unpinned against the
+reference itself.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        build()
+    return C.CDLL(str(LIB_PATH))
+
+
+_lib = _load()
+_u32 = C.c_uint32
+_vp = C.c_void_p
+
+_SIG = {
+    "orc_num_threads": (C.c_int, []),
+    "orc_set_threads": (None, [C.c_int]),
+    "orc_bfs_serial": (None, [_u32, _vp, _vp, _u32, _vp]),
+    "orc_bfs_sync_tile": (None, [_u32, _vp, _vp, _u32, _vp]),
+    "orc_verify_bfs": (C.c_int, [_u32, _vp, _vp, _u32, _vp]),
+    "orc_sssp_dijkstra": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
+    "orc_sssp_delta_serial": (None, [_u32, _vp, _vp, _vp, _u32, _u32, _vp]),
+    "orc_sssp_delta_parallel": (None, [_u32, _vp, _vp, _vp, _u32, _u32, _vp]),
+    "orc_verify_sssp": (C.c_int, [_u32, _vp, _vp, _vp, _u32, _vp]),
+    "orc_cc_union_find": (None, [_u32, _vp, _vp, _vp]),
+    "orc_cc_labelprop": (_u32, [_u32, _vp, _vp, _vp]),
+    "orc_verify_cc": (C.c_int, [_u32, _vp, _vp, _vp]),
+    "orc_pr_pull_topo_f64": (_u32, [_u32, _vp, _vp, C.c_uint64, C.c_double, C.c_double, _u32, _vp]),
+    "orc_pr_pull_topo_f32_inplace": (_u32, [_u32, _vp, _vp, C.c_uint64, C.c_float, C.c_float, _u32, _vp]),
+    "orc_pr_pull_topo_par": (_u32, [_u32, _vp, _vp, C.c_uint64, C.c_float, C.c_float, _u32, _vp]),
+    "orc_pr_pull_residual_f32": (_u32, [_u32, _vp, _vp, C.c_uint64, C.c_float, C.c_float, _u32, _vp]),
+    "orc_pr_pull_residual_f64": (_u32, [_u32, _vp, _vp, C.c_uint64, C.c_double, C.c_double, _u32, _vp]),
+    "orc_pr_push_sync_f32": (_u32, [_u32, _vp, _vp, C.c_float, C.c_float, _u32, _vp]),
+    "orc_pr_push_sync_f64": (_u32, [_u32, _vp, _vp, C.c_double, C.c_double, _u32, _vp]),
+    "orc_bc_level": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
+    "orc_bc_level_f64": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
+    "orc_bc_level_par": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
+}
+for _n, (_r, _a) in _SIG.items():
+    _f = getattr(_lib, _n)
+    _f.restype = _r
+    _f.argtypes = _a
+
+INF = 2147483646
+
+
+def _p(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def _g(g):
+    """(n, end_offs, col) of a HostCSR-like object (end_offs LC layout)."""
+    end = np.ascontiguousarray(g.end_offs, dtype=np.uint64)
+    col = np.ascontiguousarray(g.col, dtype=np.uint32)
+    return g.n, end, col
+
+
+def threads() -> int:
+    return _lib.orc_num_threads()
+
+
+def set_threads(t: int) -> None:
+    _lib.orc_set_threads(t)
+
+
+def bfs_serial(g, src: int) -> np.ndarray:
+    n, end, col = _g(g)
+    out = np.empty(n, np.uint32)
+    _lib.orc_bfs_serial(n, _p(end), _p(col), src, _p(out))
+    return out
+
+
+def bfs_sync_tile(g, src: int) -> np.ndarray:
+    n, end, col = _g(g)
+    out = np.empty(n, np.uint32)
+    _lib.orc_bfs_sync_tile(n, _p(end), _p(col), src, _p(out))
+    return out
+
+
+def verify_bfs(g, src: int, level) -> int:
+    n, end, col = _g(g)
+    lv = np.ascontiguousarray(level, np.uint32)
+    return _lib.orc_verify_bfs(n, _p(end), _p(col), src, _p(lv))
+
+
+def sssp_dijkstra(g, src: int) -> np.ndarray:
+    n, end, col = _g(g)
+    w = np.ascontiguousarray(g.w_u32, np.uint32)
+    out = np.empty(n, np.uint32)
+    _lib.orc_sssp_dijkstra(n, _p(end), _p(col), _p(w), src, _p(out))
+    return out
+
+
+def sssp_delta_serial(g, src: int, shift: int = 13) -> np.ndarray:
+    n, end, col = _g(g)
+    w = np.ascontiguousarray(g.w_u32, np.uint32)
+    out = np.empty(n, np.uint32)
+    _lib.orc_sssp_delta_serial(n, _p(end), _p(col), _p(w), src, shift, _p(out))
+    return out
+
+
+def sssp_delta_parallel(g, src: int, shift: int = 13) -> np.ndarray:
+    n, end, col = _g(g)
+    w = np.ascontiguousarray(g.w_u32, np.uint32)
+    out = np.empty(n, np.uint32)
+    _lib.orc_sssp_delta_parallel(n, _p(end), _p(col), _p(w), src, shift, _p(out))
+    return out
+
+
+def verify_sssp(g, src: int, dist) -> int:
+    n, end, col = _g(g)
+    w = np.ascontiguousarray(g.w_u32, np.uint32)
+    d = np.ascontiguousarray(dist, np.uint32)
+    return _lib.orc_verify_sssp(n, _p(end), _p(col), _p(w), src, _p(d))
+
+
+def cc_union_find(g) -> np.ndarray:
+    n, end, col = _g(g)
+    out = np.empty(n, np.uint32)
+    _lib.orc_cc_union_find(n, _p(end), _p(col), _p(out))
+    return out
+
+
+def cc_labelprop(g) -> tuple[np.ndarray, int]:
+    n, end, col = _g(g)
+    out = np.empty(n, np.uint32)
+    r = _lib.orc_cc_labelprop(n, _p(end), _p(col), _p(out))
+    return out, int(r)
+
+
+def verify_cc(g, label) -> int:
+    n, end, col = _g(g)
+    lb = np.ascontiguousarray(label, np.uint32)
+    return _lib.orc_verify_cc(n, _p(end), _p(col), _p(lb))
+
+
+def pr_pull_topo_f64(g, alpha=0.85, tol=1e-6, max_iter=1000) -> tuple[np.ndarray, int]:
+    n, end, col = _g(g)
+    out = np.empty(n, np.float64)
+    it = _lib.orc_pr_pull_topo_f64(n, _p(end), _p(col), col.size, alpha, tol, max_iter, _p(out))
+    return out, int(it)
+
+
+def pr_pull_topo_f32_inplace(g, alpha=0.85, tol=1e-6, max_iter=1000) -> tuple[np.ndarray, int]:
+    n, end, col = _g(g)
+    out = np.empty(n, np.float32)
+    it = _lib.orc_pr_pull_topo_f32_inplace(n, _p(end), _p(col), col.size, alpha, tol, max_iter, _p(out))
+    return out, int(it)
+
+
+def pr_pull_topo_par(g, alpha=0.85, tol=1e-6, max_iter=1000) -> tuple[np.ndarray, int]:
+    n, end, col = _g(g)
+    out = np.empty(n, np.float32)
+    it = _lib.orc_pr_pull_topo_par(n, _p(end), _p(col), col.size, alpha, tol, max_iter, _p(out))
+    return out, int(it)
+
+
+def pr_pull_residual(g, alpha=0.85, tol=1e-3, max_iter=1000, f64=True) -> tuple[np.ndarray, int]:
+    n, end, col = _g(g)
+    out = np.empty(n, np.float64 if f64 else np.float32)
+    fn = _lib.orc_pr_pull_residual_f64 if f64 else _lib.orc_pr_pull_residual_f32
+    it = fn(n, _p(end), _p(col), col.size, alpha, tol, max_iter, _p(out))
+    return out, int(it)
+
+
+def pr_push_sync(g, alpha=0.85, tol=1e-3, max_iter=1000, f64=True) -> tuple[np.ndarray, int]:
+    n, end, col = _g(g)
+    out = np.empty(n, np.float64 if f64 else np.float32)
+    fn = _lib.orc_pr_push_sync_f64 if f64 else _lib.orc_pr_push_sync_f32
+    it = fn(n, _p(end), _p(col), alpha, tol, max_iter, _p(out))
+    return out, int(it)
+
+
+def bc_level(g, sources, f64: bool = False, parallel: bool = False) -> np.ndarray:
+    n, end, col = _g(g)
+    src = np.ascontiguousarray(np.asarray(sources, np.uint32))
+    if f64:
+        out = np.empty(n, np.float64)
+        _lib.orc_bc_level_f64(n, _p(end), _p(col), _p(src), src.size, _p(out))
+    else:
+        out = np.empty(n, np.float32)
+        fn = _lib.orc_bc_level_par if parallel else _lib.orc_bc_level
+        fn(n, _p(end), _p(col), _p(src), src.size, _p(out))
+    return out

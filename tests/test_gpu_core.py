@@ -1,0 +1,216 @@
+"""GPU parity: BFS, SSSP, CC and PageRank kernels (through the C ABI) against
+the CPU oracle on the same seeded inputs.  Integer results are bit-exact;
+PageRank tolerances are stated per test."""
+import numpy as np
+import pytest
+
+import oracle
+from galois_b200 import (GB_CC_AFFOREST, GB_CC_LABELPROP, GB_CC_UNIONFIND, DeviceGraph, GbError, HostCSR,
+                         assign_weights_u32, erdos_renyi, grid2d, rmat)
+from galois_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+INF = oracle.INF
+
+
+def path_graph(n):
+    s = list(range(n - 1)) + list(range(1, n))
+    d = list(range(1, n)) + list(range(n - 1))
+    return HostCSR.from_edges(n, s, d)
+
+
+def star_graph(k):
+    return HostCSR.from_edges(k + 1, [0] * k + list(range(1, k + 1)), list(range(1, k + 1)) + [0] * k)
+
+
+def union(*gs):
+    """Block-diagonal union of host graphs."""
+    off = 0
+    ends, cols = [], []
+    base = 0
+    for g in gs:
+        ends.append(g.end_offs.astype(np.uint64) + np.uint64(base))
+        cols.append(g.col.astype(np.uint32) + np.uint32(off))
+        off += g.n
+        base += g.m
+    return HostCSR(np.concatenate(ends), np.concatenate(cols))
+
+
+# ---- BFS ----------------------------------------------------------------------
+
+@pytest.mark.parametrize("scale,ef", [(10, 4), (14, 16)])
+def test_bfs_rmat_sym_bit_exact(cuda_device, scale, ef):
+    g, _ = rmat(scale, ef, seed=scale)
+    deg = g.degrees()
+    with DeviceGraph(g, symmetric=True) as dg:
+        for src in (int(np.argmax(deg)), int(np.flatnonzero(deg == 1)[0]) if (deg == 1).any() else 1,
+                    int(np.flatnonzero(deg == 0)[0]) if (deg == 0).any() else 2):
+            got, st = dg.bfs(src, stats=True)
+            want = oracle.bfs_serial(g, src)
+            assert (got == want).all(), f"src {src}"
+            assert st["vertices_reached"] == int((want != INF).sum())
+
+
+def test_bfs_push_only_and_pull_heavy(cuda_device):
+    g, _ = rmat(13, 16, seed=21)
+    src = int(np.argmax(g.degrees()))
+    want = oracle.bfs_serial(g, src)
+    with DeviceGraph(g, symmetric=True) as dg:
+        dg.set_tuning(direction_opt=2)
+        got, st = dg.bfs(src, stats=True)
+        assert (got == want).all() and st["pull_rounds"] == 0
+        dg.set_tuning(direction_opt=0, do_alpha=1e6, do_beta=1e-6, heavy_degree=32, tile_edges=64)
+        got, st = dg.bfs(src, stats=True)
+        assert (got == want).all() and st["pull_rounds"] > 0
+
+
+def test_bfs_directed_push_and_transpose_pull(cuda_device):
+    g, perm = rmat(12, 8, seed=3, symmetrize=False)
+    src = int(perm[0])
+    want = oracle.bfs_serial(g, src)
+    with DeviceGraph(g, symmetric=False) as dg:
+        assert (dg.bfs(src) == want).all()
+        dg.build_transpose()
+        dg.set_tuning(do_alpha=1e6, do_beta=1e-6)
+        got, st = dg.bfs(src, stats=True)
+        assert (got == want).all()
+
+
+def test_bfs_small_shapes(cuda_device):
+    for g, src in ((path_graph(300), 0), (path_graph(300), 150), (star_graph(5000), 0), (star_graph(5000), 17),
+                   (HostCSR(np.zeros(1, np.uint64), np.zeros(0, np.uint32)), 0),
+                   (grid2d(40, 33), 0)):
+        with DeviceGraph(g, symmetric=True) as dg:
+            assert (dg.bfs(src) == oracle.bfs_serial(g, src)).all()
+
+
+def test_bfs_device_output_and_errors(cuda_device):
+    import torch
+
+    g, _ = rmat(11, 8, seed=1)
+    src = int(np.argmax(g.degrees()))
+    with DeviceGraph(g, symmetric=True) as dg:
+        out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+        dg.bfs(src, out=out)
+        torch.cuda.synchronize()
+        assert (out.cpu().numpy().view(np.uint32) == oracle.bfs_serial(g, src)).all()
+        with pytest.raises(GbError) as e:
+            dg.bfs(g.n)
+        assert e.value.status == _lib.GB_ERR_ARG
+
+
+# ---- SSSP ---------------------------------------------------------------------
+
+@pytest.mark.parametrize("shift", [0, 5, 13, 31])
+def test_sssp_rmat_directed_bit_exact(cuda_device, shift):
+    g, perm = rmat(13, 16, seed=8, symmetrize=False)
+    assign_weights_u32(g, 1, 255, seed=8)
+    src = int(perm[0])
+    with DeviceGraph(g) as dg:
+        got, st = dg.sssp(src, shift, stats=True)
+    want = oracle.sssp_dijkstra(g, src)
+    assert (got == want).all()
+    assert st["vertices_reached"] == int((want != INF).sum())
+
+
+def test_sssp_grid_many_buckets(cuda_device):
+    g = grid2d(96, 80)
+    assign_weights_u32(g, 1, 255, seed=3)
+    want = oracle.sssp_dijkstra(g, 0)
+    with DeviceGraph(g, symmetric=True) as dg:
+        for shift in (13, 8, 3):
+            got, st = dg.sssp(0, shift, stats=True)
+            assert (got == want).all()
+            if shift <= 8:
+                assert st["buckets"] > 10
+
+
+def test_sssp_heavy_tiles_and_unreachable(cuda_device):
+    g = union(star_graph(3000), path_graph(50))
+    g.w_u32 = (np.arange(g.m) % 255 + 1).astype(np.uint32)
+    with DeviceGraph(g, symmetric=True) as dg:
+        dg.set_tuning(heavy_degree=64, tile_edges=128)
+        for src in (0, 5, 3010):
+            assert (dg.sssp(src, 4) == oracle.sssp_dijkstra(g, src)).all()
+
+
+def test_sssp_needs_weights(cuda_device):
+    g, _ = rmat(8, 4, seed=1)
+    with DeviceGraph(g) as dg:
+        with pytest.raises(GbError) as e:
+            dg.sssp(0)
+        assert e.value.status == _lib.GB_ERR_ARG
+
+
+# ---- CC -----------------------------------------------------------------------
+
+@pytest.mark.parametrize("algo", [GB_CC_LABELPROP, GB_CC_UNIONFIND, GB_CC_AFFOREST])
+def test_cc_min_labels(cuda_device, algo):
+    for g in (rmat(14, 8, seed=31)[0], erdos_renyi(20000, 1.1, seed=2), union(path_graph(500), star_graph(2000)),
+              grid2d(50, 70)):
+        want = oracle.cc_union_find(g)
+        with DeviceGraph(g, symmetric=True) as dg:
+            got, st = dg.cc(algo, stats=True)
+        assert (got == want).all()
+
+
+def test_cc_directed_is_weak(cuda_device):
+    g, _ = rmat(12, 4, seed=5, symmetrize=False)
+    sym = HostCSR.from_edges(g.n, np.concatenate([np.repeat(np.arange(g.n), g.degrees()), g.col]),
+                             np.concatenate([g.col, np.repeat(np.arange(g.n), g.degrees())]))
+    want = oracle.cc_union_find(sym)
+    with DeviceGraph(g, symmetric=False) as dg:
+        for algo in (GB_CC_LABELPROP, GB_CC_UNIONFIND):
+            assert (dg.cc(algo) == want).all()
+        with pytest.raises(GbError):
+            dg.cc(GB_CC_AFFOREST)
+
+
+# ---- PageRank -------------------------------------------------------------------
+
+def test_pagerank_pull_vs_fp64(cuda_device):
+    g, _ = rmat(14, 16, seed=41)
+    want, it64 = oracle.pr_pull_topo_f64(g, 0.85, 1e-6, 1000)
+    with DeviceGraph(g, symmetric=True) as dg:
+        got, st = dg.pagerank_pull(0.85, 1e-6, 1000, stats=True)
+    # tolerance: 1e-5 L-inf (absolute), and 1e-4 relative on every vertex
+    assert np.abs(got - want).max() < 1e-5
+    assert (np.abs(got - want) / want).max() < 1e-4
+    assert abs(st["iterations"] - it64) <= 2
+
+
+def test_pagerank_pull_heavy_tiles(cuda_device):
+    g = union(star_graph(20000), path_graph(100))
+    want, it64 = oracle.pr_pull_topo_f64(g, 0.85, 1e-7, 1000)
+    with DeviceGraph(g, symmetric=True) as dg:
+        dg.set_tuning(heavy_degree=64, tile_edges=256)
+        got, st = dg.pagerank_pull(0.85, 1e-7, 1000, stats=True)
+    assert (np.abs(got - want) / want).max() < 1e-4
+
+
+def test_pagerank_pull_not_converged_status(cuda_device):
+    g, _ = rmat(10, 8, seed=2)
+    with DeviceGraph(g, symmetric=True) as dg:
+        got, st = dg.pagerank_pull(0.85, 0.0, 5, stats=True)
+        assert st["iterations"] == 5 and not st["converged"]
+        with pytest.raises(GbError) as e:
+            dg.pagerank_pull(0.85, 0.0, 5, allow_not_converged=False)
+        assert e.value.status == _lib.GB_ERR_NOT_CONVERGED
+
+
+def test_pagerank_push_vs_fp64(cuda_device):
+    g, _ = rmat(12, 8, seed=17)
+    want, _ = oracle.pr_push_sync(g, 0.85, 1e-4, 1000)
+    with DeviceGraph(g, symmetric=True) as dg:
+        got = dg.pagerank_push(0.85, 1e-4, 1000)
+    # every vertex's leftover residual is < tol and flows onward with gain
+    # alpha/(1-alpha); 2e-3 absolute covers it at tol 1e-4 on ranks of O(1)
+    assert np.abs(got - want).max() < 2e-3
+
+
+def test_pagerank_pull_residual_vs_oracle(cuda_device):
+    g, _ = rmat(12, 8, seed=19)
+    want, itw = oracle.pr_pull_residual(g, 0.85, 1e-4, 1000)
+    with DeviceGraph(g, symmetric=True) as dg:
+        got, st = dg.pagerank_pull_residual(0.85, 1e-4, 1000, stats=True)
+    assert np.abs(got - want).max() < 2e-3
