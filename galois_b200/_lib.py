@@ -53,7 +53,7 @@ class Stats(C.Structure):
     _fields_ = [("vertices_reached", C.c_uint64), ("edges_reached", C.c_uint64),
                 ("edges_scanned", C.c_uint64), ("relaxations", C.c_uint64), ("rounds", C.c_uint32),
                 ("pull_rounds", C.c_uint32), ("buckets", C.c_uint32), ("launches", C.c_uint32),
-                ("residual", C.c_double)]
+                ("residual", C.c_double), ("kernel_ms", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -286,7 +286,9 @@ int run_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats, cud
   const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
   if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_bfs: cannot size cooperative grid");
   void* args[] = {&a};
+  KernelTimer kt(stats != nullptr, s);
   GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, args, 0, s));
+  kt.stop(s);
   int* pin = static_cast<int*>(g->pinned);
   GB_CUDA(cudaMemcpyAsync(pin, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
   if (stats) {
@@ -302,6 +304,7 @@ int run_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats, cud
     stats->buckets = 0;
     stats->launches = 2;
     stats->residual = 0;
+    stats->kernel_ms = kt.ms();
   }
   if (!out_dev) {
     int st = copy_out(level_out, a.level, sizeof(uint32_t) * n, s);

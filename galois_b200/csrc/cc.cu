@@ -254,7 +254,9 @@ int run_cc(gb_graph* g, int algo, uint32_t* label_out, gb_stats* stats, cudaStre
   int aff = algo == GB_CC_AFFOREST ? 1 : 0;
   void* args_lp[] = {&a};
   void* args_uf[] = {&a, &aff};
+  KernelTimer kt(stats != nullptr, s);
   GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, algo == GB_CC_LABELPROP ? args_lp : args_uf, 0, s));
+  kt.stop(s);
   int* pin = static_cast<int*>(g->pinned);
   GB_CUDA(cudaMemcpyAsync(pin, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
   if (stats) {
@@ -267,6 +269,7 @@ int run_cc(gb_graph* g, int algo, uint32_t* label_out, gb_stats* stats, cudaStre
     stats->edges_scanned = hc->scanned;
     stats->rounds = hc->rounds;
     stats->launches = 2;
+    stats->kernel_ms = kt.ms();
   }
   if (!out_dev) {
     st = copy_out(label_out, a.p, sizeof(uint32_t) * n, s);

@@ -99,4 +99,24 @@ int copy_in(void* dst_dev, const void* src, size_t bytes, cudaStream_t stream);
 
 int ensure_transpose(gb_graph* g, cudaStream_t stream);
 
+// Times one kernel launch with CUDA events on its stream (only when `on`).
+struct KernelTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  KernelTimer(bool on, cudaStream_t s) {
+    if (on && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess) cudaEventRecord(a, s);
+  }
+  void stop(cudaStream_t s) {
+    if (b) cudaEventRecord(b, s);
+  }
+  double ms() const {
+    float t = 0.f;
+    if (a && b && cudaEventElapsedTime(&t, a, b) == cudaSuccess) return t;
+    return 0.0;
+  }
+  ~KernelTimer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
 }  // namespace gb

@@ -454,7 +454,9 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
   const int grid = coop_grid(g, kfn, kBlock, 0, t.blocks_per_sm);
   if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "pagerank: cannot size cooperative grid");
   void* args[] = {&a};
+  KernelTimer kt(stats != nullptr, s);
   GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, kBlock, args, 0, s));
+  kt.stop(s);
   PrCtl* hc = reinterpret_cast<PrCtl*>(static_cast<char*>(g->pinned) + 256);
   GB_CUDA(cudaMemcpyAsync(hc, a.ctl, sizeof(PrCtl), cudaMemcpyDeviceToHost, s));
   if (!out_dev) {
@@ -472,6 +474,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
       stats->rounds = hc->iters;
       stats->relaxations = hc->pushes;
       stats->launches = 2;
+      stats->kernel_ms = kt.ms();
       stats->residual = kind == PrKind::Pull ? (linf ? (double)bits_to_float(hc->linf[(hc->iters + 2) % 3])
                                                      : hc->l1[(hc->iters + 2) % 3])
                                              : 0.0;

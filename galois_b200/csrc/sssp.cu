@@ -302,7 +302,9 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
   if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
   void* args[] = {&a};
+  KernelTimer kt(stats != nullptr, s);
   GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, args, 0, s));
+  kt.stop(s);
   int* pin = static_cast<int*>(g->pinned);
   GB_CUDA(cudaMemcpyAsync(pin, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
   if (stats) {
@@ -322,6 +324,7 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
     stats->buckets = hc->buckets + 1;
     stats->launches = 3;
     stats->residual = 0;
+    stats->kernel_ms = kt.ms();
   }
   if (!out_dev) {
     st = copy_out(dist_out, a.dist, sizeof(uint32_t) * n, s);

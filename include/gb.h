@@ -160,6 +160,8 @@ typedef struct gb_stats {
   uint32_t buckets;          /* delta buckets processed (SSSP)               */
   uint32_t launches;         /* kernels launched by this call                */
   double residual;           /* final L1 residual (PageRank)                 */
+  double kernel_ms;          /* device time of the main (persistent) kernel,
+                                CUDA events on the launching stream          */
 } gb_stats;
 
 /* Tuning knobs; zero fields mean "library default / autotuned". */
