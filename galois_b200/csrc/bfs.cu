@@ -326,3 +326,155 @@ extern "C" int gb_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* 
   GB_CUDA(cudaSetDevice(g->device));
   return gb::run_bfs(g, src, level_out, stats, static_cast<cudaStream_t>(stream), nullptr, 0);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free BFS.
+//
+// Some callers cannot call cudaMalloc: a host application that owns and
+// budgets every byte of device memory itself and forbids libraries from
+// allocating behind its back, or code that must not take the allocator's
+// implicit device synchronisation in the middle of its work.  For them,
+// gb_bfs_noalloc runs the same BFS kernels as gb_bfs, but takes the graph as
+// caller-owned device arrays (no gb_graph handle, which allocates) and keeps
+// its frontier queues, bitmaps and control words in the fixed-size file-scope
+// array below.  Every GPU that loads libgb holds that array until the process
+// exits.
+//
+// Limits: n <= kNoAllocMaxNodes (2^20) vertices and m <= kNoAllocMaxArcs
+// (2^26) arcs; larger graphs are rejected with GB_ERR_CAPACITY.
+// All calls on a device share the one array and it keeps the previous call's
+// contents, so each call clears what must start at zero (the control block;
+// bitmaps and levels are rewritten by the init kernel).  Calls that overlap
+// on the GPU (other streams, other host threads) race on the array and must
+// be serialised by the caller.
+// The first call on a device looks up the array's device address with
+// cudaGetSymbolAddress (with that device current); make that first call
+// before any stream capture on the device.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace gb {
+namespace {
+
+constexpr uint32_t kNoAllocMaxNodes = 1u << 20;
+constexpr uint64_t kNoAllocMaxArcs = 1ull << 26;
+constexpr uint32_t kNoAllocHeavy = 512;
+constexpr uint32_t kNoAllocTile = 512;
+
+constexpr size_t na_round(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t na_tile_cap() {
+  return kNoAllocMaxArcs / kNoAllocTile + kNoAllocMaxArcs / (kNoAllocHeavy + 1) + 2;
+}
+// control block + validation flag + visited + 3 frontier bitmaps + 2 light
+// queues + 2 tile queues, each rounded to 256 bytes like Carver does
+constexpr size_t kNoAllocScratchBytes =
+    na_round(sizeof(BfsCtl)) + na_round(sizeof(int)) + 4 * na_round(sizeof(uint32_t) * (kNoAllocMaxNodes / 32)) +
+    2 * na_round(sizeof(uint32_t) * kNoAllocMaxNodes) + 2 * na_round(sizeof(uint2) * na_tile_cap());
+
+static __device__ __align__(256) unsigned char g_bfs_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+void* g_noalloc_addr[kMaxDevices] = {};
+std::mutex g_noalloc_mu;
+
+// Device address of the scratch array for the current device (looked up once
+// per device; host code must never pass the symbol itself to a kernel).
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  GB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) GB_FAIL(GB_ERR_UNSUPPORTED, "gb_bfs_noalloc: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_bfs_noalloc_scratch);
+    if (e != cudaSuccess || !p) return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return GB_OK;
+}
+
+__global__ void noalloc_validate(const uint64_t* __restrict__ offs, const uint32_t* __restrict__ col, uint32_t n,
+                                 uint64_t m, int* bad) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  if (tid == 0 && (offs[0] != 0 || offs[n] != m)) atomicOr(bad, 1);
+  for (uint64_t v = tid; v < n; v += stride)
+    if (offs[v] > offs[v + 1]) atomicOr(bad, 1);
+  for (uint64_t e = tid; e < m; e += stride)
+    if (col[e] >= n) atomicOr(bad, 2);
+}
+
+}  // namespace
+}  // namespace gb
+
+extern "C" int gb_bfs_noalloc(const uint64_t* offs, const uint32_t* col, uint32_t n, uint64_t m, int symmetric,
+                              uint32_t src, uint32_t* level_out, void* stream) {
+  using namespace gb;
+  clear_error();
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!offs || !col || !level_out) GB_FAIL(GB_ERR_ARG, "gb_bfs_noalloc: null argument");
+  if (n == 0 || src >= n) GB_FAIL(GB_ERR_ARG, "gb_bfs_noalloc: source %u not below n %u", src, n);
+  if (n > kNoAllocMaxNodes || m > kNoAllocMaxArcs)
+    GB_FAIL(GB_ERR_CAPACITY, "gb_bfs_noalloc: graph of %u vertices / %llu arcs exceeds the fixed scratch "
+            "(at most %u vertices and %llu arcs); use gb_bfs", n, (unsigned long long)m, kNoAllocMaxNodes,
+            (unsigned long long)kNoAllocMaxArcs);
+  if (!is_device_ptr(offs) || !is_device_ptr(col) || !is_device_ptr(level_out))
+    GB_FAIL(GB_ERR_ARG, "gb_bfs_noalloc: offs, col and level_out must be device memory");
+  void* base = nullptr;
+  int st = noalloc_scratch(&base);
+  if (st != GB_OK) return st;
+  const uint32_t words = (n + 31) / 32;
+  const FrontierLayout fl = frontier_layout(n, m, kNoAllocHeavy, kNoAllocTile);
+  const size_t need = carve_size<BfsCtl>(1) + carve_size<int>(1) + 4 * carve_size<uint32_t>(words) + fl.bytes;
+  if (need > kNoAllocScratchBytes) GB_FAIL(GB_ERR_CAPACITY, "gb_bfs_noalloc: scratch too small (%zu > %zu)", need,
+                                           kNoAllocScratchBytes);
+  Carver cv(base);
+  BfsArgs a{};
+  a.ctl = cv.take<BfsCtl>(1);
+  int* bad = cv.take<int>(1);
+  a.visited = cv.take<uint32_t>(words);
+  for (int i = 0; i < 3; ++i) a.fbits[i] = cv.take<uint32_t>(words);
+  a.fq = carve_frontier(cv, fl);
+  a.level = level_out;
+  a.offs = offs;
+  a.col = col;
+  if (symmetric) {
+    a.in_offs = offs;
+    a.in_col = col;
+  }
+  a.n = n;
+  a.m = m;
+  a.src = src;
+  a.heavy = kNoAllocHeavy;
+  a.tile = kNoAllocTile;
+  a.alpha = 15.f;
+  a.beta = 18.f;
+  a.max_levels = n + 1;
+  int dev = 0, sms = 0;
+  GB_CUDA(cudaGetDevice(&dev));
+  GB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  // the array keeps the previous call's contents: clear the control block and
+  // the validation flag (bitmaps and levels are rewritten by bfs_init)
+  GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(BfsCtl), s));
+  GB_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+  noalloc_validate<<<sms * 4, 256, 0, s>>>(offs, col, n, m, bad);
+  GB_CUDA(cudaGetLastError());
+  int hbad = 0;
+  GB_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  GB_CUDA(cudaStreamSynchronize(s));
+  if (hbad) GB_FAIL(GB_ERR_FORMAT, "gb_bfs_noalloc: invalid CSR (offsets not monotone / not ending at m, or id >= n)");
+  bfs_init<<<sms * 4, 256, 0, s>>>(a);
+  GB_CUDA(cudaGetLastError());
+  const void* kfn = reinterpret_cast<const void*>(&bfs_persistent<256>);
+  int per_sm = 0;
+  GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, 256, 0));
+  if (per_sm <= 0) GB_FAIL(GB_ERR_CUDA, "gb_bfs_noalloc: cannot size cooperative grid");
+  void* args[] = {&a};
+  GB_CUDA(cudaLaunchCooperativeKernel(kfn, per_sm * sms, 256, args, 0, s));
+  int herr = 0;
+  GB_CUDA(cudaMemcpyAsync(&herr, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  GB_CUDA(cudaStreamSynchronize(s));
+  if (herr) return dev_err_status(herr, "gb_bfs_noalloc");
+  return GB_OK;
+}

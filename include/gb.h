@@ -182,6 +182,19 @@ int gb_graph_get_tuning(const gb_graph* g, gb_tuning* t);
 int gb_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats,
            void* stream);
 
+/* Allocation-free BFS (no counterpart in the reference).  For callers that
+ * cannot call cudaMalloc -- e.g. a host application that owns and budgets all
+ * device memory and forbids libraries from allocating -- this runs the gb_bfs
+ * kernels over caller-owned device arrays (offs: n+1 begin offsets, col: m
+ * ids, level_out: n) with all scratch in a fixed file-scope device array that
+ * every GPU loading libgb keeps until exit.  Limits: n <= 2^20, m <= 2^26
+ * (GB_ERR_CAPACITY beyond).  Calls share the array: calls that overlap on the
+ * GPU race.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  symmetric != 0 allows bottom-up steps. */
+int gb_bfs_noalloc(const uint64_t* offs, const uint32_t* col, uint32_t n,
+                   uint64_t m, int symmetric, uint32_t src,
+                   uint32_t* level_out, void* stream);
+
 /* Delta-stepping SSSP over uint32 weights (SSSP.cpp:118-173, -delta is a
  * shift: bucket = dist >> delta_shift).  dist_out[n]. */
 int gb_sssp_delta(gb_graph* g, uint32_t src, uint32_t delta_shift,
