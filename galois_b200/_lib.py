@@ -62,7 +62,7 @@ class Stats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("heavy_degree", C.c_uint32), ("tile_edges", C.c_uint32), ("block_threads", C.c_uint32),
                 ("blocks_per_sm", C.c_uint32), ("do_alpha", C.c_float), ("do_beta", C.c_float),
-                ("direction_opt", C.c_int)]
+                ("direction_opt", C.c_int), ("local_depth", C.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -156,44 +156,38 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(BfsArgs a) {
     if (!pull) {
       const uint32_t* qin = a.fq.light[L & 1];
       const uint2* tin = a.fq.tiles[L & 1];
-      // light vertices, 32 per warp grab
-      for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&cur.light_work, 32u);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= q_light) break;
-        const uint32_t idx = base + lane;
-        uint64_t b = 0;
-        uint32_t d = 0;
-        if (idx < q_light) {
-          const uint32_t v = qin[idx];
-          b = ldg(a.offs + v);
-          d = (uint32_t)(ldg(a.offs + v + 1) - b);
-        }
-        my_scanned += d;
-        warp_expand(b, d, 0u, [&](bool valid, uint64_t e, uint32_t, uint32_t) {
-          const uint32_t u = valid ? ldg(a.col + e) : 0u;
-          discover(valid, u);
-        });
-      }
-      // heavy vertices' edge tiles, one tile per warp grab
-      for (;;) {
-        uint32_t t = 0;
-        if (lane == 0) t = atomicAdd(&cur.tile_work, 1u);
-        t = __shfl_sync(kFull, t, 0);
-        if (t >= q_tiles) break;
-        const uint2 tv = tin[t];
-        const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
-        const uint64_t b = vb + (uint64_t)tv.y * a.tile;
-        const uint64_t e_end = min(ve, b + a.tile);
-        if (lane == 0) my_scanned += e_end - b;
-        for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
-          const uint64_t e = e0 + lane;
-          const bool valid = e < e_end;
-          const uint32_t u = valid ? ldg(a.col + e) : 0u;
-          discover(valid, u);
-        }
-      }
+      // light vertices 32 per task, heavy vertices' edge tiles one per task,
+      // spread statically over all warps (no work-grabbing atomics)
+      for_each_frontier_task(
+          q_light, q_tiles, gtid >> 5, gthreads >> 5,
+          [&](uint32_t base, uint32_t vpt) {
+            const uint32_t idx = base + lane;
+            uint64_t b = 0;
+            uint32_t d = 0;
+            if (lane < vpt && idx < q_light) {
+              const uint32_t v = qin[idx];
+              b = ldg(a.offs + v);
+              d = (uint32_t)(ldg(a.offs + v + 1) - b);
+            }
+            my_scanned += d;
+            warp_expand(b, d, 0u, [&](bool valid, uint64_t e, uint32_t, uint32_t) {
+              const uint32_t u = valid ? ldg(a.col + e) : 0u;
+              discover(valid, u);
+            });
+          },
+          [&](uint32_t t) {
+            const uint2 tv = tin[t];
+            const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
+            const uint64_t b = vb + (uint64_t)tv.y * a.tile;
+            const uint64_t e_end = min(ve, b + a.tile);
+            if (lane == 0) my_scanned += e_end - b;
+            for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
+              const uint64_t e = e0 + lane;
+              const bool valid = e < e_end;
+              const uint32_t u = valid ? ldg(a.col + e) : 0u;
+              discover(valid, u);
+            }
+          });
     } else {
       // bottom-up over all vertices; warp-uniform trip count
       for (uint64_t base = gtid - lane; base < a.n; base += gthreads) {

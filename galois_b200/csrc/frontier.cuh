@@ -68,14 +68,14 @@ __device__ __forceinline__ void seed_vertex(const FrontierQueues& q, int qb, Fro
   }
 }
 
-// Warp-collective: append every lane's discovered vertex `u` (disc == true)
-// into queue buffer qb, binned by degree; zero-degree vertices are counted but
-// not queued (they have nothing to expand).  All 32 lanes must call.
-__device__ __forceinline__ void push_discovered(const FrontierQueues& q, int qb, FrontierCounters& c,
-                                                bool disc, uint32_t u, const uint64_t* __restrict__ offs,
-                                                uint32_t heavy, uint32_t tile, int* err) {
-  uint64_t d = 0;
-  if (disc) d = __ldg(offs + u + 1) - __ldg(offs + u);
+// Warp-collective: append every lane's discovered vertex `u` (disc == true,
+// out-degree d) into queue buffer qb, binned by degree; zero-degree vertices
+// are counted but not queued (nothing to expand).  kCount also maintains the
+// vertex and degree totals the BFS direction heuristic reads.  All 32 lanes
+// must call.
+template <bool kCount>
+__device__ __forceinline__ void push_with_degree(const FrontierQueues& q, int qb, FrontierCounters& c, bool disc,
+                                                 uint32_t u, uint64_t d, uint32_t heavy, uint32_t tile, int* err) {
   const bool light = disc && d > 0 && d <= heavy;
   const bool hv = disc && d > heavy;
   warp_push(light, u, q.light[qb], &c.light, q.light_cap, err);
@@ -88,13 +88,52 @@ __device__ __forceinline__ void push_discovered(const FrontierQueues& q, int qb,
       else raise_err(err, kDevOverflow);
     }
   }
-  const unsigned dmask = __ballot_sync(kFull, disc);
-  if (dmask) {
-    const unsigned long long ds = warp_sum((unsigned long long)d);
-    if (lane_id() == 0) {
-      atomicAdd(&c.vertices, (uint32_t)__popc(dmask));
-      if (ds) atomicAdd(&c.degree_sum, ds);
+  if (kCount) {
+    const unsigned dmask = __ballot_sync(kFull, disc);
+    if (dmask) {
+      const unsigned long long ds = warp_sum((unsigned long long)(disc ? d : 0));
+      if (lane_id() == 0) {
+        atomicAdd(&c.vertices, (uint32_t)__popc(dmask));
+        if (ds) atomicAdd(&c.degree_sum, ds);
+      }
     }
+  }
+}
+
+template <bool kCount = true>
+__device__ __forceinline__ void push_discovered(const FrontierQueues& q, int qb, FrontierCounters& c, bool disc,
+                                                uint32_t u, const uint64_t* __restrict__ offs, uint32_t heavy,
+                                                uint32_t tile, int* err) {
+  uint64_t d = 0;
+  if (disc) d = __ldg(offs + u + 1) - __ldg(offs + u);
+  push_with_degree<kCount>(q, qb, c, disc, u, d, heavy, tile, err);
+}
+
+// Vertices per light task: 32 when the frontier fills every warp, fewer
+// (a power of two) for small frontiers so that more warps share them and the
+// per-phase critical path is one expansion step instead of several.
+__device__ __forceinline__ uint32_t vertices_per_task(uint32_t q_light, uint64_t nwarps) {
+  const uint64_t per = q_light / (nwarps ? nwarps : 1);
+  if (per >= 32) return 32;
+  uint32_t k = 1;
+  while ((uint64_t)(k << 1) <= per) k <<= 1;
+  return k;
+}
+
+// Static, atomic-free distribution of a frontier over all warps of the grid:
+// tasks [0, nchunks) are `vpt`-entry chunks of the light queue (vpt from
+// vertices_per_task), the remaining tasks are heavy-vertex tiles; warp w
+// takes tasks w, w + nwarps, ...  chunk(base, vpt) / tile(t) are called by
+// whole warps; in a chunk, lanes < vpt own entries base + lane.
+template <class ChunkFn, class TileFn>
+__device__ __forceinline__ void for_each_frontier_task(uint32_t q_light, uint32_t q_tiles, uint64_t gwarp,
+                                                       uint64_t nwarps, ChunkFn&& chunk, TileFn&& tile) {
+  const uint32_t vpt = vertices_per_task(q_light, nwarps);
+  const uint64_t nchunks = ((uint64_t)q_light + vpt - 1) / vpt;
+  const uint64_t total = nchunks + q_tiles;
+  for (uint64_t t = gwarp; t < total; t += nwarps) {
+    if (t < nchunks) chunk((uint32_t)(t * vpt), vpt);
+    else tile((uint32_t)(t - nchunks));
   }
 }
 

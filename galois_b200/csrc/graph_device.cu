@@ -55,11 +55,14 @@ int ws_reserve(gb_graph* g, size_t bytes, cudaStream_t stream) {
 
 gb_tuning effective_tuning(const gb_graph* g) {
   gb_tuning t = g->tuning;
-  if (!t.heavy_degree) t.heavy_degree = 512;
-  if (!t.tile_edges) t.tile_edges = 512;
-  if (!t.block_threads) t.block_threads = 256;
+  if (!t.heavy_degree) t.heavy_degree = 128;
+  if (!t.tile_edges) t.tile_edges = 256;
+  if (!t.block_threads) t.block_threads = 1024;  // SSSP persistent CTA (1 per SM: cheap barrier)
   if (t.do_alpha <= 0.f) t.do_alpha = 15.f;  // bfsDirectionOpt.cpp:68-72
   if (t.do_beta <= 0.f) t.do_beta = 18.f;    // bfsDirectionOpt.cpp:73-77
+  // local relaxation rounds pay off on low-degree, high-diameter graphs
+  // (grids, road-like) and cost on power-law graphs
+  if (t.local_depth == 0) t.local_depth = g->max_degree <= 32 ? 8 : -1;
   return t;
 }
 

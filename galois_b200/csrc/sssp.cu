@@ -9,14 +9,18 @@
 // B200 design: one cooperative persistent launch.  OBIM becomes
 //   * a near queue (light vertices + heavy-vertex edge tiles, frontier.cuh)
 //     holding vertices whose tentative distance lies in the current bucket;
-//     duplicate pushes within a phase are filtered by a per-vertex phase stamp;
+//     a per-vertex stamp keeps a vertex in at most one queue per phase;
+//   * per-warp local queues in shared memory: a warp keeps relaxing light
+//     vertices it improved itself for up to `local_depth` rounds inside the
+//     same phase (label-correcting inside the bucket), so high-diameter
+//     graphs need far fewer grid-wide phases; leftovers go to the near queue;
 //   * a far pile holding vertices relaxed beyond the bucket (membership
 //     bitmap, so each vertex is in the pile at most once).
-// A phase relaxes every near vertex with its CURRENT distance (no stale
-// items); when the near queue drains, the far pile is split: settled entries
-// are dropped, the minimum remaining bucket becomes current (empty buckets
-// are skipped), its vertices move to the near queue and the rest are
-// compacted.  Phases are separated by a bounded grid barrier.
+// Work is spread over warps statically (no work-grabbing atomics).  When the
+// near queue drains, the far pile is split: settled entries are dropped, the
+// minimum remaining bucket becomes current (empty buckets are skipped), its
+// vertices move to the near queue and the rest are compacted.  Phases are
+// separated by the bounded grid barrier.
 
 #include "device_common.cuh"
 #include "device_graph.cuh"
@@ -25,6 +29,9 @@
 namespace gb {
 
 namespace {
+
+constexpr int kLocalQ = 64;  // local-queue entries per warp
+constexpr uint32_t kNotQueued = 0xFFFFFFFFu;
 
 struct SsspCtl {
   GridBar bar;
@@ -48,7 +55,7 @@ struct SsspArgs {
   uint32_t src;
   uint32_t shift;
   uint32_t* dist;
-  uint32_t* stamp;  // phase in which the vertex was last queued (near)
+  uint32_t* stamp;  // phase whose queue holds the vertex, kNotQueued if none
   uint32_t* infar;  // bitmap: vertex currently in the far pile
   uint32_t* far[2];
   FrontierQueues fq;
@@ -56,6 +63,8 @@ struct SsspArgs {
   uint32_t heavy;
   uint32_t tile;
   uint32_t max_phases;
+  int local_depth;
+  int all_light;  // max degree <= heavy: skip the degree lookup when queueing
 };
 
 __global__ void sssp_init(SsspArgs a) {
@@ -64,7 +73,7 @@ __global__ void sssp_init(SsspArgs a) {
   const uint32_t words = (a.n + 31) >> 5;
   for (uint64_t v = tid; v < a.n; v += stride) {
     a.dist[v] = (v == a.src) ? 0u : kInf;
-    a.stamp[v] = (v == a.src) ? 0u : 0xFFFFFFFFu;
+    a.stamp[v] = (v == a.src) ? 0u : kNotQueued;
   }
   for (uint64_t w = tid; w < words; w += stride) a.infar[w] = 0;
   if (tid == 0) {
@@ -78,12 +87,16 @@ __global__ void sssp_init(SsspArgs a) {
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
+  __shared__ uint32_t s_lq[BLOCK / 32][kLocalQ];
   SsspCtl* ctl = a.ctl;
   const unsigned nblocks = gridDim.x;
   const uint64_t deadline = kernel_deadline();
   const uint32_t lane = lane_id();
   const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
   const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  uint32_t* lq = s_lq[threadIdx.x >> 5];
   unsigned long long my_scanned = 0, my_relax = 0;
 
   uint32_t bucket = 0;  // current bucket index; near items have dist < hi
@@ -107,40 +120,59 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
     const uint64_t hi64 = ((uint64_t)bucket + 1) << a.shift;
     const uint32_t hi = hi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)hi64;
     uint32_t* farq = a.far[fp];
-
-    // relax one arc; all lanes call (warp collectives inside)
-    auto relax = [&](bool valid, uint32_t u, uint32_t nd) {
-      bool to_near = false, to_far = false;
-      if (valid && nd < a.dist[u]) {
-        const uint32_t old = atomicMin(&a.dist[u], nd);
-        if (nd < old) {
-          ++my_relax;
-          if (nd < hi) {
-            if (a.stamp[u] != next_stamp) to_near = atomicExch(&a.stamp[u], next_stamp) != next_stamp;
-          } else {
-            const uint32_t bit = 1u << (u & 31);
-            if (!(a.infar[u >> 5] & bit)) to_far = !(atomicOr(&a.infar[u >> 5], bit) & bit);
-          }
-        }
-      }
-      push_discovered(a.fq, (P + 1) & 1, nxt, to_near, u, a.offs, a.heavy, a.tile, &ctl->err);
-      warp_push(to_far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
-    };
+    const int qnext = (P + 1) & 1;
 
     if (q_light != 0 || q_tiles != 0) {
       // ---- relaxation phase --------------------------------------------
-      const uint32_t* qin = a.fq.light[P & 1];
-      const uint2* tin = a.fq.tiles[P & 1];
-      for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&cur.light_work, 32u);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= q_light) break;
-        const uint32_t idx = base + lane;
+      uint32_t lq_n = 0;  // warp-uniform local queue length
+      // Route improved vertices: light ones into this warp's local queue
+      // while it has room (and local rounds are enabled), the rest into the
+      // near queue; beyond-bucket ones into the far pile.  All lanes call.
+      auto route = [&](bool to_near, bool to_far, uint32_t u) {
+        uint64_t d = 0;
+        // when every vertex is light the exact degree is not needed to bin
+        // it: 1 stands for "light, non-empty" (an empty vertex expands to
+        // nothing, so queueing it costs one idle lane)
+        if (to_near) d = a.all_light ? 1 : ldg(a.offs + u + 1) - ldg(a.offs + u);
+        bool loc = a.local_depth > 0 && to_near && d > 0 && d <= a.heavy;
+        const unsigned lm = __ballot_sync(kFull, loc);
+        const uint32_t k = __popc(lm);
+        if (k) {
+          if (lq_n + k <= (uint32_t)kLocalQ) {
+            if (loc) lq[lq_n + __popc(lm & lanemask_lt)] = u;
+            lq_n += k;
+            __syncwarp();
+          } else {
+            loc = false;
+          }
+        }
+        push_with_degree<false>(a.fq, qnext, nxt, to_near && !loc, u, d, a.heavy, a.tile, &ctl->err);
+        warp_push(to_far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
+      };
+      auto relax = [&](bool valid, uint32_t u, uint32_t nd) {
+        bool to_near = false, to_far = false;
+        if (valid && nd < a.dist[u]) {
+          const uint32_t old = atomicMin(&a.dist[u], nd);
+          if (nd < old) {
+            ++my_relax;
+            if (nd < hi) {
+              // fence: the dist update is visible before the stamp is read
+              // (pairs with the fence after a local pop resets the stamp)
+              if (a.local_depth > 0) __threadfence();
+              if (a.stamp[u] != next_stamp) to_near = atomicExch(&a.stamp[u], next_stamp) != next_stamp;
+            } else {
+              const uint32_t bit = 1u << (u & 31);
+              if (!(a.infar[u >> 5] & bit)) to_far = !(atomicOr(&a.infar[u >> 5], bit) & bit);
+            }
+          }
+        }
+        route(to_near, to_far, u);
+      };
+      // expand one light vertex per lane (has == false: idle lane)
+      auto expand = [&](bool has, uint32_t v) {
         uint64_t b = 0;
         uint32_t d = 0, dv = 0;
-        if (idx < q_light) {
-          const uint32_t v = qin[idx];
+        if (has) {
           b = ldg(a.offs + v);
           d = (uint32_t)(ldg(a.offs + v + 1) - b);
           dv = a.dist[v];
@@ -154,28 +186,55 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
           }
           relax(valid, u, nd);
         });
-      }
-      for (;;) {
-        uint32_t t = 0;
-        if (lane == 0) t = atomicAdd(&cur.tile_work, 1u);
-        t = __shfl_sync(kFull, t, 0);
-        if (t >= q_tiles) break;
-        const uint2 tv = tin[t];
-        const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
-        const uint64_t b = vb + (uint64_t)tv.y * a.tile;
-        const uint64_t e_end = min(ve, b + a.tile);
-        const uint32_t dsrc = a.dist[tv.x];
-        if (lane == 0) my_scanned += e_end - b;
-        for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
-          const uint64_t e = e0 + lane;
-          const bool valid = e < e_end;
-          uint32_t u = 0, nd = 0;
-          if (valid) {
-            u = ldg(a.col + e);
-            nd = dsrc + ldg(a.w + e);
-          }
-          relax(valid, u, nd);
+      };
+      const uint32_t* qin = a.fq.light[P & 1];
+      const uint2* tin = a.fq.tiles[P & 1];
+      for_each_frontier_task(
+          q_light, q_tiles, gwarp, nwarps,
+          [&](uint32_t base, uint32_t vpt) {
+            const uint32_t idx = base + lane;
+            const bool has = lane < vpt && idx < q_light;
+            expand(has, has ? qin[idx] : 0u);
+          },
+          [&](uint32_t t) {
+            const uint2 tv = tin[t];
+            const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
+            const uint64_t b = vb + (uint64_t)tv.y * a.tile;
+            const uint64_t e_end = min(ve, b + a.tile);
+            const uint32_t dsrc = a.dist[tv.x];
+            if (lane == 0) my_scanned += e_end - b;
+            for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
+              const uint64_t e = e0 + lane;
+              const bool valid = e < e_end;
+              uint32_t u = 0, nd = 0;
+              if (valid) {
+                u = ldg(a.col + e);
+                nd = dsrc + ldg(a.w + e);
+              }
+              relax(valid, u, nd);
+            }
+          });
+      // local rounds: keep relaxing what this warp improved (LIFO)
+      for (int r = 0; r < a.local_depth && lq_n > 0; ++r) {
+        const uint32_t take = min(32u, lq_n);
+        const bool has = lane < take;
+        const uint32_t v = has ? lq[lq_n - take + lane] : 0u;
+        __syncwarp();
+        lq_n -= take;
+        if (has) {
+          a.stamp[v] = kNotQueued;  // from here an improvement re-queues v
+          __threadfence();
         }
+        expand(has, v);
+      }
+      // leftovers go to the near queue; they keep their stamp P+1
+      while (lq_n > 0) {
+        const uint32_t take = min(32u, lq_n);
+        const bool has = lane < take;
+        const uint32_t v = has ? lq[lq_n - take + lane] : 0u;
+        __syncwarp();
+        lq_n -= take;
+        push_discovered<false>(a.fq, qnext, nxt, has, v, a.offs, a.heavy, a.tile, &ctl->err);
       }
       if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
       ++P;
@@ -223,7 +282,7 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
           }
           if (!keep) atomicAnd(&a.infar[u >> 5], ~(1u << (u & 31)));
         }
-        push_discovered(a.fq, (P + 1) & 1, nxt, to_near, u, a.offs, a.heavy, a.tile, &ctl->err);
+        push_discovered<false>(a.fq, qnext, nxt, to_near, u, a.offs, a.heavy, a.tile, &ctl->err);
         warp_push(keep, u, keepq, &ctl->far_count[fp ^ 1], a.n, &ctl->err);
       }
     }
@@ -295,15 +354,20 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   a.heavy = t.heavy_degree;
   a.tile = t.tile_edges;
   a.max_phases = 0x7FFFFFFFu;
+  a.local_depth = t.local_depth < 0 ? 0 : t.local_depth;
+  a.all_light = g->max_degree <= t.heavy_degree ? 1 : 0;
   GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), s));
   sssp_init<<<g->sm_count * 4, 256, 0, s>>>(a);
   GB_CUDA(cudaGetLastError());
-  const void* kfn = reinterpret_cast<const void*>(&sssp_persistent<256>);
-  const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
+  const bool big = t.block_threads >= 1024;
+  const int block = big ? 1024 : 256;
+  const void* kfn = big ? reinterpret_cast<const void*>(&sssp_persistent<1024>)
+                        : reinterpret_cast<const void*>(&sssp_persistent<256>);
+  const int grid = coop_grid(g, kfn, block, 0, t.blocks_per_sm);
   if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
   void* args[] = {&a};
   KernelTimer kt(stats != nullptr, s);
-  GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, args, 0, s));
+  GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, block, args, 0, s));
   kt.stop(s);
   int* pin = static_cast<int*>(g->pinned);
   GB_CUDA(cudaMemcpyAsync(pin, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -315,15 +379,14 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
     GB_CUDA(cudaMemcpyAsync(hc, a.ctl, sizeof(SsspCtl), cudaMemcpyDeviceToHost, s));
     GB_CUDA(cudaMemcpyAsync(hr, reach, 16, cudaMemcpyDeviceToHost, s));
     GB_CUDA(cudaStreamSynchronize(s));
+    *stats = gb_stats{};
     stats->vertices_reached = hr[0];
     stats->edges_reached = hr[1];
     stats->edges_scanned = hc->scanned;
     stats->relaxations = hc->relax;
     stats->rounds = hc->phases;
-    stats->pull_rounds = 0;
     stats->buckets = hc->buckets + 1;
-    stats->launches = 3;
-    stats->residual = 0;
+    stats->launches = 2;
     stats->kernel_ms = kt.ms();
   }
   if (!out_dev) {

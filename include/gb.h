@@ -173,6 +173,8 @@ typedef struct gb_tuning {
   float do_alpha;        /* push->pull switch (bfsDirectionOpt.cpp:68-72)  */
   float do_beta;         /* pull->push switch (bfsDirectionOpt.cpp:73-77)  */
   int direction_opt;     /* 0 = pull steps allowed when in-edges exist, 2 = push only */
+  int local_depth;       /* SSSP: per-warp local-queue rounds per phase
+                            (0 = library default, < 0 = off) */
 } gb_tuning;
 int gb_graph_set_tuning(gb_graph* g, const gb_tuning* t);
 int gb_graph_get_tuning(const gb_graph* g, gb_tuning* t);

@@ -113,16 +113,29 @@ def test_sssp_rmat_directed_bit_exact(cuda_device, shift):
     assert st["vertices_reached"] == int((want != INF).sum())
 
 
-def test_sssp_grid_many_buckets(cuda_device):
+@pytest.mark.parametrize("local_depth,block", [(-1, 256), (8, 256), (64, 1024)])
+def test_sssp_grid_many_buckets(cuda_device, local_depth, block):
     g = grid2d(96, 80)
     assign_weights_u32(g, 1, 255, seed=3)
     want = oracle.sssp_dijkstra(g, 0)
     with DeviceGraph(g, symmetric=True) as dg:
+        dg.set_tuning(local_depth=local_depth, block_threads=block)
         for shift in (13, 8, 3):
             got, st = dg.sssp(0, shift, stats=True)
             assert (got == want).all()
             if shift <= 8:
                 assert st["buckets"] > 10
+
+
+def test_sssp_local_queues_rmat(cuda_device):
+    g, perm = rmat(14, 16, seed=12, symmetrize=False)
+    assign_weights_u32(g, 1, 255, seed=12)
+    src = int(perm[0])
+    want = oracle.sssp_dijkstra(g, src)
+    with DeviceGraph(g) as dg:
+        for depth in (1, 32, 256):
+            dg.set_tuning(local_depth=depth)
+            assert (dg.sssp(src, 13) == want).all()
 
 
 def test_sssp_heavy_tiles_and_unreachable(cuda_device):
