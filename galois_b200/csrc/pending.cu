@@ -3,9 +3,6 @@
 
 extern "C" {
 
-int gb_bc(gb_graph*, const uint32_t*, uint32_t, uint32_t, float*, gb_stats*, void*) {
-  GB_FAIL(GB_ERR_UNSUPPORTED, "gb_bc: not built");
-}
 int gb_multi_graph_bfs_cc(gb_graph*, const uint32_t*, uint32_t, const uint32_t*, uint32_t*, uint32_t*,
                           gb_stats*, void*) {
   GB_FAIL(GB_ERR_UNSUPPORTED, "gb_multi_graph_bfs_cc: not built");
