@@ -71,7 +71,7 @@ __global__ void bfs_init(BfsArgs a) {
     a.fbits[1][w] = 0;
     a.fbits[2][w] = 0;
   }
-  if (tid == 0) {
+  if (tid == 0 && a.src < a.n) {  // src == ~0u: seeded by bfs_seed_many
     const uint64_t b = a.offs[a.src], d = a.offs[a.src + 1] - b;
     FrontierCounters& c = a.ctl->fc[0];
     c.vertices = 1;
@@ -308,6 +308,81 @@ int run_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats, cud
     GB_CUDA(cudaStreamSynchronize(s));
     if (*pin) return dev_err_status(*pin, "gb_bfs");
   }
+  return GB_OK;
+}
+
+namespace {
+
+// Seeds level 0 with k sources at once (a BFS from a virtual super-source):
+// for disjoint graphs packed block-diagonally this gives every graph its own
+// BFS levels in one traversal.  Repeated sources are queued once.
+__global__ void bfs_seed_many(BfsArgs a, const uint32_t* __restrict__ srcs, uint32_t k) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  FrontierCounters& c = a.ctl->fc[0];
+  for (uint64_t base = tid - lane_id(); base < k; base += stride) {
+    const uint64_t i = base + lane_id();
+    bool first = false;
+    uint32_t s = 0;
+    if (i < k) {
+      s = srcs[i];
+      const uint32_t bit = 1u << (s & 31);
+      first = !(atomicOr(&a.visited[s >> 5], bit) & bit);
+      if (first) {
+        a.level[s] = 0;
+        atomicOr(&a.fbits[0][s >> 5], bit);
+      }
+    }
+    push_discovered<true>(a.fq, 0, c, first, s, a.offs, a.heavy, a.tile, &a.ctl->err);
+  }
+}
+
+}  // namespace
+
+// BFS from k sources (device array) into a device level array, asynchronous
+// on `s` (no host synchronisation, so it can be captured in a CUDA graph once
+// the workspace exists).  Errors raised on the device are returned by the
+// next synchronous call on the handle.
+int run_bfs_sources(gb_graph* g, const uint32_t* d_srcs, uint32_t k, uint32_t* d_level, cudaStream_t s) {
+  const gb_tuning t = effective_tuning(g);
+  const uint32_t n = g->n;
+  const uint32_t words = (n + 31) / 32;
+  FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
+  const size_t need = carve_size<BfsCtl>(1) + 4 * carve_size<uint32_t>(words) + fl.bytes;
+  int st = ws_reserve(g, need, s);
+  if (st != GB_OK) return st;
+  Carver cv(g->ws);
+  BfsArgs a{};
+  a.ctl = cv.take<BfsCtl>(1);
+  a.visited = cv.take<uint32_t>(words);
+  for (int i = 0; i < 3; ++i) a.fbits[i] = cv.take<uint32_t>(words);
+  a.fq = carve_frontier(cv, fl);
+  a.level = d_level;
+  a.offs = g->offs;
+  a.col = g->col;
+  if (t.direction_opt != 2 && g->symmetric) {
+    a.in_offs = g->offs;
+    a.in_col = g->col;
+  }
+  a.n = n;
+  a.m = g->m;
+  a.src = 0xFFFFFFFFu;
+  a.heavy = t.heavy_degree;
+  a.tile = t.tile_edges;
+  a.alpha = t.do_alpha;
+  a.beta = t.do_beta;
+  a.max_levels = n + 1;
+  GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(BfsCtl), s));
+  bfs_init<<<g->sm_count * 4, 256, 0, s>>>(a);
+  bfs_seed_many<<<std::max<uint32_t>(1, std::min<uint32_t>((k + 255) / 256, g->sm_count * 4)), 256, 0, s>>>(a, d_srcs, k);
+  GB_CUDA(cudaGetLastError());
+  const void* kfn = reinterpret_cast<const void*>(&bfs_persistent<256>);
+  const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
+  if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "bfs: cannot size cooperative grid");
+  void* args[] = {&a};
+  GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, args, 0, s));
+  // keep the device error word where the caller can read it
+  GB_CUDA(cudaMemcpyAsync(static_cast<int*>(g->pinned) + 8, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
   return GB_OK;
 }
 

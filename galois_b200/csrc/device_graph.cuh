@@ -43,6 +43,14 @@ struct gb_graph {
   uint32_t sweep_nheavy = 0;
   uint32_t sweep_heavy = 0;
   uint32_t sweep_tile = 0;
+  // multi-graph (block-diagonal) layout, validated once and cached
+  uint32_t* mg_first = nullptr;   // device copy of graph_first [ngraphs+1]
+  uint32_t* mg_src = nullptr;     // device global sources [ngraphs]
+  uint32_t* mg_level = nullptr;   // device outputs used for host-pointer calls
+  uint32_t* mg_label = nullptr;
+  uint32_t* mg_stage = nullptr;   // pinned staging of host arrays
+  uint32_t mg_ngraphs = 0;
+  uint64_t mg_hash = 0;
   // scratch workspace, grown on demand
   void* ws = nullptr;
   size_t ws_bytes = 0;

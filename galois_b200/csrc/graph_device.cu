@@ -318,6 +318,13 @@ int gb_graph_free(gb_graph* g) {
   cudaFree(g->t_emap);
   cudaFree(g->outdeg_of_stored);
   cudaFree(g->colsum);
+  cudaFree(g->sweep_tiles);
+  cudaFree(g->sweep_heavy_list);
+  cudaFree(g->mg_first);
+  cudaFree(g->mg_src);
+  cudaFree(g->mg_level);
+  cudaFree(g->mg_label);
+  if (g->mg_stage) cudaFreeHost(g->mg_stage);
   cudaFree(g->ws);
   if (g->pinned) cudaFreeHost(g->pinned);
   delete g;

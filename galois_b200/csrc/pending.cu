@@ -3,10 +3,6 @@
 
 extern "C" {
 
-int gb_multi_graph_bfs_cc(gb_graph*, const uint32_t*, uint32_t, const uint32_t*, uint32_t*, uint32_t*,
-                          gb_stats*, void*) {
-  GB_FAIL(GB_ERR_UNSUPPORTED, "gb_multi_graph_bfs_cc: not built");
-}
 int gb_ppr_forward(gb_graph*, uint32_t, const float*, float, float, uint32_t, float*, uint32_t*, gb_stats*,
                    void*) {
   GB_FAIL(GB_ERR_UNSUPPORTED, "gb_ppr_forward: not built");

@@ -175,6 +175,22 @@ def _free_ptr(p) -> None:
     libc.free(C.cast(p, C.c_void_p))
 
 
+def pack_graphs(graphs: list) -> tuple[HostCSR, np.ndarray]:
+    """Block-diagonal packing of disjoint graphs; returns (graph, graph_first)
+    with graph_first[k] the first vertex of graph k and graph_first[-1] = n."""
+    first = np.zeros(len(graphs) + 1, dtype=np.uint32)
+    ends, cols = [], []
+    vbase, ebase = 0, 0
+    for k, g in enumerate(graphs):
+        first[k] = vbase
+        ends.append(g.end_offs.astype(np.uint64) + np.uint64(ebase))
+        cols.append(g.col.astype(np.uint32) + np.uint32(vbase))
+        vbase += g.n
+        ebase += g.m
+    first[-1] = vbase
+    return HostCSR(np.concatenate(ends), np.concatenate(cols)), first
+
+
 def transpose(g: HostCSR) -> tuple[HostCSR, np.ndarray]:
     """Transposed graph and, per transposed arc, its index in g."""
     emap = np.empty(g.m, dtype=np.uint64)

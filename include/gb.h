@@ -249,10 +249,14 @@ int gb_bc(gb_graph* g, const uint32_t* srcs, uint32_t nsrc, uint32_t batch,
           float* bc_out, gb_stats* stats, void* stream);
 
 /* Many disjoint graphs in one launch: the graphs are packed block-diagonally
- * into `g` (vertex ranges graph_first[k] .. graph_first[k+1]-1, k < ngraphs),
- * BFS runs from graph_first[k] + local_src[k] for every k at once and CC
- * labels every graph.  Labels are local ids (min local id of the component),
- * levels are per-graph BFS levels.  level_out/label_out: [n]. */
+ * into a symmetric `g` (vertex ranges graph_first[k] .. graph_first[k+1]-1,
+ * graph_first has ngraphs+1 HOST entries, graph_first[ngraphs] == n, no arc
+ * leaves its range), BFS runs from graph_first[k] + local_src[k] (host array)
+ * for every k at once and CC labels every graph.  Labels are local ids (min
+ * local id of the component), levels are per-graph BFS levels.
+ * level_out/label_out: [n] (either may be NULL).  The first call on a layout
+ * validates it; later calls with device outputs issue only stream-ordered
+ * work, so they can be captured in a CUDA graph. */
 int gb_multi_graph_bfs_cc(gb_graph* g, const uint32_t* graph_first,
                           uint32_t ngraphs, const uint32_t* local_src,
                           uint32_t* level_out, uint32_t* label_out,
