@@ -123,10 +123,10 @@ SIGNATURES: dict[str, tuple] = {
                                             C.POINTER(Stats), _vp]),
     "gb_bc": (C.c_int, [_gp, _vp, C.c_uint32, C.c_uint32, _vp, C.POINTER(Stats), _vp]),
     "gb_multi_graph_bfs_cc": (C.c_int, [_gp, _vp, C.c_uint32, _vp, _vp, _vp, C.POINTER(Stats), _vp]),
-    "gb_ppr_forward": (C.c_int, [_gp, C.c_uint32, _vp, C.c_float, C.c_float, C.c_uint32, _vp, _u32p,
+    "gb_ppr_forward": (C.c_int, [_gp, C.c_uint32, _vp, _vp, C.c_float, C.c_float, C.c_uint32, _vp, _u32p,
                                  C.POINTER(Stats), _vp]),
-    "gb_ppr_backward": (C.c_int, [_gp, C.c_uint32, _vp, _vp, C.c_float, C.c_float, C.c_uint32, _vp, _vp,
-                                  _u32p, C.POINTER(Stats), _vp]),
+    "gb_ppr_backward": (C.c_int, [_gp, C.c_uint32, _vp, _vp, _vp, C.c_float, C.c_float, C.c_uint32, _vp,
+                                  _vp, _u32p, C.POINTER(Stats), _vp]),
     "gb_autotune": (C.c_int, [_gp, C.c_char_p, C.c_uint32, C.c_char_p, C.POINTER(Tuning), _vp]),
 }
 

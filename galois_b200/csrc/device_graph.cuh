@@ -51,6 +51,9 @@ struct gb_graph {
   uint32_t* mg_stage = nullptr;   // pinned staging of host arrays
   uint32_t mg_ngraphs = 0;
   uint64_t mg_hash = 0;
+  // personalised-PageRank state (opaque, owned by ppr.cu)
+  void* ppr_state = nullptr;
+  void (*ppr_free)(gb_graph*) = nullptr;
   // scratch workspace, grown on demand
   void* ws = nullptr;
   size_t ws_bytes = 0;

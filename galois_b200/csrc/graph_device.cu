@@ -318,6 +318,7 @@ int gb_graph_free(gb_graph* g) {
   cudaFree(g->t_emap);
   cudaFree(g->outdeg_of_stored);
   cudaFree(g->colsum);
+  if (g->ppr_free) g->ppr_free(g);
   cudaFree(g->sweep_tiles);
   cudaFree(g->sweep_heavy_list);
   cudaFree(g->mg_first);

@@ -32,6 +32,32 @@ __global__ void sweep_tiles_kernel(const uint64_t* __restrict__ offs, uint32_t n
 
 }  // namespace
 
+int build_row_schedule(const uint64_t* offs, uint32_t n, uint64_t m, uint32_t heavy, uint32_t tile, int sm_count,
+                       void* pinned, cudaStream_t s, uint2** tiles, uint32_t** heavy_list, uint32_t* ntiles,
+                       uint32_t* nheavy) {
+  const uint64_t tc64 = m / tile + m / ((uint64_t)heavy + 1) + 2;
+  const uint32_t tile_cap = (uint32_t)std::min<uint64_t>(tc64, 0xFFFFFFF0ull);
+  const uint32_t heavy_cap = (uint32_t)std::min<uint64_t>(m / ((uint64_t)heavy + 1) + 2, 0xFFFFFFF0ull);
+  *tiles = nullptr;
+  *heavy_list = nullptr;
+  GB_CUDA(cudaMalloc(tiles, sizeof(uint2) * tile_cap));
+  GB_CUDA(cudaMalloc(heavy_list, sizeof(uint32_t) * heavy_cap));
+  uint32_t* dcount = nullptr;
+  GB_CUDA(cudaMalloc(&dcount, 16));
+  GB_CUDA(cudaMemsetAsync(dcount, 0, 16, s));
+  sweep_tiles_kernel<<<sm_count * 4, 256, 0, s>>>(offs, n, heavy, tile, *tiles, tile_cap, *heavy_list, heavy_cap,
+                                                   dcount, reinterpret_cast<int*>(dcount + 2));
+  uint32_t* h = static_cast<uint32_t*>(pinned);
+  cudaMemcpyAsync(h, dcount, 16, cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  cudaFree(dcount);
+  if (e != cudaSuccess) return cuda_fail(e, "row schedule");
+  if (h[2]) GB_FAIL(GB_ERR_CAPACITY, "row schedule overflow");
+  *ntiles = h[0];
+  *nheavy = h[1];
+  return GB_OK;
+}
+
 int ensure_sweep_schedule(gb_graph* g, uint32_t heavy, uint32_t tile, cudaStream_t s, SweepSched* out) {
   if (!(g->sweep_tiles && g->sweep_heavy == heavy && g->sweep_tile == tile)) {
     cudaFree(g->sweep_tiles);

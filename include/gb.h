@@ -262,24 +262,29 @@ int gb_multi_graph_bfs_cc(gb_graph* g, const uint32_t* graph_first,
                           uint32_t* level_out, uint32_t* label_out,
                           gb_stats* stats, void* stream);
 
-/* Personalised PageRank, batched over B teleport vectors, on a directed graph
- * with positive float edge weights w (arc j->i).  W~ = w / colsum (column-
- * normalised by source out-weight).  Solves x = (1-alpha) T + alpha W~ x by
- * Jacobi iteration to max-column L1 change <= tol.
- *   teleport: dense [n][B] row-major float (device or host)
- *   x_out:    [n][B] row-major float
- * The graph needs gb_graph_build_transpose (done on first use). */
-int gb_ppr_forward(gb_graph* g, uint32_t B, const float* teleport, float alpha,
-                   float tol, uint32_t max_iter, float* x_out,
-                   uint32_t* iters_out, gb_stats* stats, void* stream);
+/* Personalised PageRank (no counterpart in the reference; an addition beside
+ * the PageRank kernels), batched over B teleport vectors, on a directed graph
+ * with positive float arc weights w (arc j->i, CSR order).  W~_ij = w_ji / s_j
+ * with s_j the out-weight sum of j.  Solves x = (1-alpha) T + alpha W~ x by
+ * Jacobi iteration from x0 = (1-alpha) T until the largest per-column L1
+ * change is <= tol (or max_iter).
+ *   B:        1, or a multiple of 4 up to 128
+ *   teleport: dense [n][B] row-major float, device memory
+ *   w:        [m] device floats, or NULL for the uploaded w_f32
+ *   x_out:    [n][B] row-major float, device memory
+ * The transpose is built on first use. */
+int gb_ppr_forward(gb_graph* g, uint32_t B, const float* teleport,
+                   const float* w, float alpha, float tol, uint32_t max_iter,
+                   float* x_out, uint32_t* iters_out, gb_stats* stats,
+                   void* stream);
 /* Adjoint of gb_ppr_forward: given x (forward solution) and gx = dL/dx, solves
- * (I - alpha W~)^T lam = gx and returns
+ * lam = gx + alpha W~^T lam (Jacobi, same stopping rule) and returns
  *   grad_teleport[n][B] = (1-alpha) lam
- *   grad_w[m]           = dL/dw for every arc (summed over the batch),
- *                         through the column normalisation.
- * Either output may be NULL. */
+ *   grad_w[m]  = dL/dw_ji = alpha/s_j * sum_b x_j^b (lam_i^b - mu_j^b),
+ *                mu_j = (lam_j - gx_j)/alpha, summed over the batch
+ * Either output may be NULL; all arrays are device memory. */
 int gb_ppr_backward(gb_graph* g, uint32_t B, const float* x, const float* gx,
-                    float alpha, float tol, uint32_t max_iter,
+                    const float* w, float alpha, float tol, uint32_t max_iter,
                     float* grad_teleport, float* grad_w, uint32_t* iters_out,
                     gb_stats* stats, void* stream);
 
