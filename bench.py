@@ -39,7 +39,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--app", choices=["sssp", "bfs", "cc", "pr"], default="sssp")
+    ap.add_argument("--app", choices=["sssp", "bfs", "cc", "pr", "bc", "multigraph", "ppr"], default="sssp")
     ap.add_argument("--small", action="store_true", help="reduced sizes (profiling / smoke only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -350,6 +350,191 @@ class PrJob(Job):
 
 
 JOBS = {"sssp": SsspJob, "bfs": BfsJob, "cc": CcJob, "pr": PrJob}
+BATCHED = ("bc", "multigraph", "ppr")
+
+
+def _time_gpu(fn, steps: int) -> float:
+    """Device time (ms) of `steps` calls of fn on torch's current stream."""
+    import torch
+
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(steps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_batched(args) -> None:
+    """Batched kernels against looping the plain kernels on the same GPU."""
+    import torch
+
+    import oracle
+    from galois_b200 import DeviceGraph, erdos_renyi, rmat
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    steps, warm = args.steps, args.warmup
+    line = {"n_gpus": 1, "steps": steps, "warmup": warm, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic (seeded generators)"}
+    clocks = ClockSampler(dev)
+    if args.app == "bc":
+        scale = 14 if args.small else 20
+        g, _ = rmat(scale, 16, seed=20, symmetrize=True)
+        rng = np.random.default_rng(1024)
+        srcs = rng.choice(np.flatnonzero(g.degrees() > 0), 1024, replace=False).astype(np.uint32)
+        dg = DeviceGraph(g, symmetric=True, device=dev)
+        # traversed edges: forward + backward over the arcs of reached vertices, per source
+        lv = torch.empty(g.n, dtype=torch.int32, device="cuda")
+        m_r = sum(dg.bfs(int(s), out=lv, stats=True)[1]["edges_reached"] for s in srcs)
+        units = 2.0 * m_r
+        out = torch.empty(g.n, dtype=torch.float32, device="cuda")
+        dg.bc(srcs, batch=64, out=out)
+        for _ in range(warm):
+            dg.bc(srcs, batch=64, out=out)
+        clocks.start()
+        t_b = _time_gpu(lambda: dg.bc(srcs, batch=64, out=out), steps)
+        dg.bc(srcs, batch=1, out=out)
+        t_l = _time_gpu(lambda: dg.bc(srcs, batch=1, out=out), 1)
+        clk = clocks.stop()
+        bc_gpu = out.cpu().numpy()
+        sample = srcs[:8]
+        with DeviceGraph(g, symmetric=True, device=dev) as dg8:
+            got8 = dg8.bc(sample, batch=8)
+        ref8 = oracle.bc_level(g, sample, f64=True)
+        rel = float((np.abs(got8 - ref8) / np.maximum(np.abs(ref8), 1.0)).max())
+        t0 = time.perf_counter()
+        oracle.bc_level(g, srcs[:16], parallel=True)
+        t_cpu = time.perf_counter() - t0
+        m_r16 = units * 16 / len(srcs)
+        line.update({"metric": "BC aggregate GTEPS (fwd+bwd arcs of reached vertices, 1024 sources)",
+                     "unit": "GTEPS", "dtype": "f64 sigma / f32 dependency", "value": units * steps / (t_b / 1e3) / 1e9,
+                     "ms_per_step": t_b / steps,
+                     "config": {"workload": f"Brandes BC, RMAT-{scale} sym ef16, 1024 seeded sources, 64 per launch",
+                                "n": g.n, "m": g.m},
+                     "looped": {"value": units / (t_l / 1e3) / 1e9, "ms_per_step": t_l,
+                                "how": "gb_bc batch=1: one persistent single-source launch per source"},
+                     "speedup_vs_looped": (t_l) / (t_b / steps),
+                     "parity": f"max rel err vs FP64 oracle on 8 sources: {rel:.2e}",
+                     "cpu_baseline": {"value": m_r16 / t_cpu / 1e9, "unit": "GTEPS", "cores": oracle.threads(),
+                                      "kind": "port", "sample": "16 of the 1024 sources, Level BC, OpenMP"},
+                     "clocks": clk, "gpu_launches": 3 * (len(srcs) // 64) + 1})
+        dg.free()
+    elif args.app == "multigraph":
+        from galois_b200.graph import pack_graphs
+
+        k = 64 if args.small else 512
+        hi = 20000 if args.small else 200000
+        rng = np.random.default_rng(512)
+        sizes = np.exp(rng.uniform(np.log(1000), np.log(hi), k)).astype(int)
+        graphs = [erdos_renyi(int(n), 8.0, seed=100 + i) for i, n in enumerate(sizes)]
+        packed, first = pack_graphs(graphs)
+        local = np.zeros(k, np.uint32)
+        dg = DeviceGraph(packed, symmetric=True, device=dev)
+        dg.autotune("bfs", int(first[0]))
+        lv = torch.empty(packed.n, dtype=torch.int32, device="cuda")
+        lb = torch.empty(packed.n, dtype=torch.int32, device="cuda")
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            dg.multi_graph_bfs_cc(first, local, lv, lb)
+            torch.cuda.synchronize()
+            cg = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(cg, stream=s):
+                dg.multi_graph_bfs_cc(first, local, lv, lb)
+        for _ in range(warm):
+            cg.replay()
+        clocks.start()
+        t_b = _time_gpu(cg.replay, steps)
+        # looped: one handle per graph, gb_bfs + gb_cc each
+        dgs = [DeviceGraph(gk, symmetric=True, device=dev) for gk in graphs]
+        outs = [(torch.empty(gk.n, dtype=torch.int32, device="cuda"), torch.empty(gk.n, dtype=torch.int32, device="cuda"))
+                for gk in graphs]
+
+        def loop():
+            for d, (a, b) in zip(dgs, outs):
+                d.bfs(0, out=a)
+                d.cc(1, out=b)
+
+        loop()
+        t_l = _time_gpu(loop, 1)
+        clk = clocks.stop()
+        lvh = lv.cpu().numpy().view(np.uint32)
+        lbh = lb.cpu().numpy().view(np.uint32)
+        ok = all(np.array_equal(lvh[first[i]:first[i + 1]], oracle.bfs_serial(graphs[i], 0)) and
+                 np.array_equal(lbh[first[i]:first[i + 1]], oracle.cc_union_find(graphs[i]))
+                 for i in range(0, k, max(1, k // 16)))
+        units = 2.0 * packed.m  # BFS over the reached arcs (giant components) + CC over every arc
+        t0 = time.perf_counter()
+        for i in range(0, k, max(1, k // 16)):
+            oracle.bfs_sync_tile(graphs[i], 0)
+            oracle.cc_labelprop(graphs[i])
+        t_cpu = time.perf_counter() - t0
+        cpu_units = 2.0 * sum(graphs[i].m for i in range(0, k, max(1, k // 16)))
+        line.update({"metric": "multi-graph BFS+CC throughput (graphs per second)", "unit": "graphs/s", "dtype": "u32",
+                     "value": k * steps / (t_b / 1e3), "ms_per_step": t_b / steps,
+                     "aggregate_gteps": units * steps / (t_b / 1e3) / 1e9,
+                     "config": {"workload": f"{k} Erdos-Renyi graphs, n log-uniform in [1000, {hi}], mean degree 8, "
+                                            "BFS from local vertex 0 + CC, one CUDA-graph replay per step",
+                                "n": packed.n, "m": packed.m},
+                     "looped": {"value": k / (t_l / 1e3), "ms_per_step": t_l,
+                                "how": "one handle per graph: gb_bfs + gb_cc per graph"},
+                     "speedup_vs_looped": t_l / (t_b / steps),
+                     "parity": "bit-exact on sampled graphs" if ok else "MISMATCH",
+                     "cpu_baseline": {"value": cpu_units / t_cpu / 1e9, "unit": "GTEPS", "cores": oracle.threads(),
+                                      "kind": "port", "sample": "every k/16-th graph: SyncTile BFS + LabelProp CC"},
+                     "clocks": clk, "gpu_launches": 9 * steps})
+        del cg
+        for d in dgs:
+            d.free()
+        dg.free()
+    else:  # ppr
+        from galois_b200 import assign_weights_f32
+        from galois_b200.ppr import ppr
+
+        scale = 16 if args.small else 22
+        g, _ = rmat(scale, 16, seed=22, symmetrize=False)
+        assign_weights_f32(g, seed=22)
+        B = 128
+        rng = np.random.default_rng(128)
+        T = torch.zeros((g.n, B), dtype=torch.float32, device="cuda")
+        for b in range(B):
+            T[torch.from_numpy(rng.choice(g.n, 32, replace=False)).cuda(), b] = 1.0 / 32
+        c = torch.from_numpy(rng.standard_normal((g.n, B)).astype(np.float32)).cuda()
+        dg = DeviceGraph(g, device=dev)
+        w = torch.from_numpy(g.w_f32).cuda().requires_grad_(True)
+
+        def batched():
+            w.grad = None
+            x = ppr(dg, T, w, 0.85, 1e-7)
+            (c * x).sum().backward()
+
+        def looped():
+            w.grad = None
+            for b in range(B):
+                x = ppr(dg, T[:, b:b + 1].contiguous(), w, 0.85, 1e-7)
+                (c[:, b:b + 1] * x).sum().backward()
+
+        batched()
+        for _ in range(warm):
+            batched()
+        clocks.start()
+        t_b = _time_gpu(batched, steps)
+        looped()
+        t_l = _time_gpu(looped, 1)
+        clk = clocks.stop()
+        line.update({"metric": "PPR forward+adjoint columns per second (batch 128, tol 1e-7)", "unit": "columns/s",
+                     "dtype": "f32", "value": B * steps / (t_b / 1e3), "ms_per_step": t_b / steps,
+                     "config": {"workload": f"personalised PageRank + adjoint, RMAT-{scale} directed ef16, w~U(0,1], "
+                                            "128 teleports x 32 nonzeros, alpha 0.85, tol 1e-7, loss sum(c*x)",
+                                "n": g.n, "m": g.m},
+                     "looped": {"value": B / (t_l / 1e3), "ms_per_step": t_l,
+                                "how": "128 single-column solves (B=1 kernels), forward+adjoint each"},
+                     "speedup_vs_looped": t_l / (t_b / steps), "clocks": clk, "gpu_launches": 12 * steps})
+        dg.free()
+    emit(line)
 
 
 def cpu_units(job: Job, gpu_stats: list) -> float:
@@ -403,8 +588,17 @@ def run_reference(args, job_cls) -> None:
 
 def main() -> None:
     args = parse_args()
-    job_cls = JOBS[args.app]
     rank = int(os.environ.get("RANK", "0"))
+    if args.app in BATCHED:
+        if args.impl == "reference":
+            if rank == 0:
+                emit({"impl": "reference", "unavailable": f"--app {args.app}: the CPU baseline is reported inside the "
+                                                          "GPU line (cpu_baseline); see the default SSSP workload"})
+            return
+        if rank == 0:
+            run_batched(args)
+        return
+    job_cls = JOBS[args.app]
     if args.impl == "reference":
         if rank == 0:
             run_reference(args, job_cls)
