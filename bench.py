@@ -40,10 +40,15 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--app", choices=["sssp", "bfs", "cc", "pr", "bc", "multigraph", "ppr"], default="sssp")
-    ap.add_argument("--small", action="store_true", help="reduced sizes (profiling / smoke only)")
+    ap.add_argument("--size", choices=["small", "medium", "full"], default="full",
+                    help="graph sizes: full = the benchmark configuration; medium/small for profiling")
+    ap.add_argument("--small", action="store_true", help="same as --size small")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.small:
+        args.size = "small"
+    return args
 
 
 # ---------------------------------------------------------------- plumbing --
@@ -168,6 +173,10 @@ def pinned_copy(a: np.ndarray) -> np.ndarray:
 _PINNED: list = []
 
 
+def pick(size: str, small, medium, full):
+    return {"small": small, "medium": medium, "full": full}[size]
+
+
 def emit(line: dict) -> None:
     print(json.dumps(line), flush=True)
 
@@ -182,8 +191,8 @@ class Job:
     kernel = ""
     workload = ""
 
-    def __init__(self, small: bool):
-        self.small = small
+    def __init__(self, size: str):
+        self.size = size
         self.graphs = []  # dicts: name, host (HostCSR), symmetric, src
 
     def device_call(self, dg, gi, out):
@@ -218,11 +227,11 @@ class SsspJob(Job):
     kernel = "sssp_persistent"
     workload = "SSSP delta-stepping, delta=2^13, w~U[1,255]: RMAT-22 directed ef16 (src = generator vertex 0) + grid 4096x4096 (src 0)"
 
-    def __init__(self, small):
-        super().__init__(small)
+    def __init__(self, size):
+        super().__init__(size)
         from galois_b200 import assign_weights_u32, grid2d, rmat
 
-        scale, side = (16, 512) if small else (22, 4096)
+        scale, side = pick(size, (16, 512), (20, 2048), (22, 4096))
         g, perm = rmat(scale, 16, seed=22, symmetrize=False)
         assign_weights_u32(g, 1, 255, seed=22)
         self.graphs.append({"name": f"rmat{scale}-directed", "host": g, "symmetric": False, "src": int(perm[0])})
@@ -251,11 +260,11 @@ class BfsJob(Job):
     kernel = "bfs_persistent"
     workload = "BFS from the max-degree vertex, RMAT-20 symmetric ef16"
 
-    def __init__(self, small):
-        super().__init__(small)
+    def __init__(self, size):
+        super().__init__(size)
         from galois_b200 import rmat
 
-        scale = 16 if small else 20
+        scale = pick(size, 16, 18, 20)
         g, _ = rmat(scale, 16, seed=20, symmetrize=True)
         self.graphs.append({"name": f"rmat{scale}-sym", "host": g, "symmetric": True,
                             "src": int(np.argmax(g.degrees()))})
@@ -280,11 +289,11 @@ class CcJob(Job):
     kernel = "cc_labelprop"
     workload = "CC label propagation + pointer jumping, RMAT-24 symmetric ef16, min-id labels"
 
-    def __init__(self, small):
-        super().__init__(small)
+    def __init__(self, size):
+        super().__init__(size)
         from galois_b200 import rmat
 
-        scale = 18 if small else 24
+        scale = pick(size, 18, 21, 24)
         g, _ = rmat(scale, 16, seed=24, symmetrize=True)
         self.graphs.append({"name": f"rmat{scale}-sym", "host": g, "symmetric": True, "src": 0})
 
@@ -312,11 +321,11 @@ class PrJob(Job):
     dtype = "f32"
     workload = "PageRank pull-topological, alpha 0.85, tol 1e-6 (L1), max 1000, RMAT-24 symmetric ef16"
 
-    def __init__(self, small):
-        super().__init__(small)
+    def __init__(self, size):
+        super().__init__(size)
         from galois_b200 import rmat
 
-        scale = 18 if small else 24
+        scale = pick(size, 18, 21, 24)
         g, _ = rmat(scale, 16, seed=24, symmetrize=True)
         self.graphs.append({"name": f"rmat{scale}-sym", "host": g, "symmetric": True, "src": 0})
         self.iters = {}
@@ -382,7 +391,7 @@ def run_batched(args) -> None:
             "vs_baseline": None, "data": "synthetic (seeded generators)"}
     clocks = ClockSampler(dev)
     if args.app == "bc":
-        scale = 14 if args.small else 20
+        scale = pick(args.size, 14, 17, 20)
         g, _ = rmat(scale, 16, seed=20, symmetrize=True)
         rng = np.random.default_rng(1024)
         srcs = rng.choice(np.flatnonzero(g.degrees() > 0), 1024, replace=False).astype(np.uint32)
@@ -426,8 +435,8 @@ def run_batched(args) -> None:
     elif args.app == "multigraph":
         from galois_b200.graph import pack_graphs
 
-        k = 64 if args.small else 512
-        hi = 20000 if args.small else 200000
+        k = pick(args.size, 64, 128, 512)
+        hi = pick(args.size, 20000, 50000, 200000)
         rng = np.random.default_rng(512)
         sizes = np.exp(rng.uniform(np.log(1000), np.log(hi), k)).astype(int)
         graphs = [erdos_renyi(int(n), 8.0, seed=100 + i) for i, n in enumerate(sizes)]
@@ -494,7 +503,7 @@ def run_batched(args) -> None:
         from galois_b200 import assign_weights_f32
         from galois_b200.ppr import ppr
 
-        scale = 16 if args.small else 22
+        scale = pick(args.size, 16, 19, 22)
         g, _ = rmat(scale, 16, seed=22, symmetrize=False)
         assign_weights_f32(g, seed=22)
         B = 128
@@ -545,7 +554,7 @@ def run_reference(args, job_cls) -> None:
     """CPU restatement of the reference algorithm on all host cores (rank 0 only)."""
     import oracle
 
-    job = job_cls(args.small)
+    job = job_cls(args.size)
     # units per step: the same traversed-edge count the GPU arm reports,
     # computed on the host from the CPU result (reached vertices' degrees)
     t0 = time.perf_counter()
@@ -611,7 +620,7 @@ def main() -> None:
     dist = Dist(want_pg=True)
     dev = dist.local_rank
     torch.cuda.set_device(dev)
-    job = job_cls(args.small)
+    job = job_cls(args.size)
     tname, npdt = job.out_kind()
     dgs, outs = [], []
     for g in job.graphs:
@@ -647,7 +656,7 @@ def main() -> None:
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_src, "kernel": job.kernel,
                 "algorithmic_bytes_per_step": bytes_step, "kernel_ms_per_step": sum(kms),
-                "traffic": traffic_from_profiles(f"{args.app}{'-small' if args.small else ''}")}
+                "traffic": traffic_from_profiles(f"{args.app}-{args.size}")}
     line = {"metric": job.metric, "value": value, "unit": job.unit, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": job.dtype, "data": "synthetic (seeded generators)",
