@@ -122,9 +122,25 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
         }
       }
     };
-    sweep_all(
+    // 4 steps of (column, label) loads in flight per lane
+    sweep_all_mlp<4, uint32_t>(
         a.offs, a.n, a.sched, gwarp, nwarps,
-        [&](bool valid, uint64_t e, uint32_t, uint32_t v) { hook(valid, v, valid ? ldg(a.col + e) : 0u); },
+        [&](bool valid, uint64_t e, uint32_t v) {
+          const uint32_t u = valid ? ldg(a.col + e) : 0u;
+          return (valid && (!a.half || u > v)) ? u : 0xFFFFFFFFu;
+        },
+        [&](bool, uint64_t, uint32_t u, uint32_t) { return u != 0xFFFFFFFFu ? a.p[u] : 0u; },
+        [&](bool, uint32_t, uint32_t v, uint32_t u, uint32_t pu) {
+          if (u == 0xFFFFFFFFu) return;
+          const uint32_t pv = a.p[v];
+          if (pv != pu) {
+            const uint32_t hi = max(pv, pu), lo = min(pv, pu);
+            if (lo < a.p[hi]) {
+              atomicMin(&a.p[hi], lo);
+              my_change = true;
+            }
+          }
+        },
         [&](uint32_t, bool, bool) {},
         [&](uint32_t v, uint64_t b, uint64_t e) {
           if (lane == 0) my_scanned += e - b;

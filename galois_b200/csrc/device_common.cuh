@@ -175,6 +175,56 @@ __device__ __forceinline__ void warp_expand(uint64_t beg, uint32_t deg, uint32_t
   }
 }
 
+// warp_expand with U steps in flight: for U consecutive 32-arc steps the
+// owners are resolved first, then every step's first load (load1: e.g. the
+// column id) is issued, then every step's dependent load (load2: e.g. the
+// gathered value), and only then consume() runs per step in order.  Each lane
+// keeps U independent memory chains in flight instead of one.
+//   load1(valid, edge, owner_payload) -> uint32_t
+//   load2(valid, edge, v1, owner_payload) -> T
+//   consume(valid, owner_lane, owner_payload, v1, v2)   (all lanes call)
+template <int U, class T, class Load1, class Load2, class Consume>
+__device__ __forceinline__ void warp_expand_mlp(uint64_t beg, uint32_t deg, uint32_t payload, Load1&& load1,
+                                                Load2&& load2, Consume&& consume) {
+  const unsigned lane = lane_id();
+  uint32_t incl = deg;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, incl, o);
+    if ((int)lane >= o) incl += t;
+  }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  const uint32_t excl = incl - deg;
+  for (uint32_t base = 0; base < total; base += 32 * U) {
+    uint32_t pos[U], opl[U], v1[U];
+    uint64_t edge[U];
+    bool valid[U];
+    T v2[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const uint32_t e = base + 32 * k + lane;
+      uint32_t p = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t v = __shfl_sync(kFull, incl, p + step - 1);
+        if (v <= e) p += step;
+      }
+      pos[k] = p;
+      const uint64_t ob = __shfl_sync(kFull, beg, p);
+      const uint32_t oex = __shfl_sync(kFull, excl, p);
+      opl[k] = __shfl_sync(kFull, payload, p);
+      valid[k] = e < total;
+      edge[k] = ob + (uint64_t)(e - oex);
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) v1[k] = load1(valid[k], edge[k], opl[k]);
+#pragma unroll
+    for (int k = 0; k < U; ++k) v2[k] = load2(valid[k], edge[k], v1[k], opl[k]);
+#pragma unroll
+    for (int k = 0; k < U; ++k) consume(valid[k], pos[k], opl[k], v1[k], v2[k]);
+  }
+}
+
 // Read-only cached loads for graph arrays that no kernel writes.
 template <class T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }

@@ -136,10 +136,12 @@ __global__ void __launch_bounds__(kBlock) pr_pull_persistent(PrArgs a) {
       my_l1 += (double)fabsf(value - old);
       my_max = fmaxf(my_max, fabsf(value - old));
     };
-    sweep_all(
+    // 4 steps of (column id, contribution) loads in flight per lane
+    sweep_all_mlp<4, float>(
         a.offs, a.n, a.sched, gwarp, nwarps,
-        [&](bool valid, uint64_t e, uint32_t owner, uint32_t) {
-          float x = valid ? c_in[ldg(a.col + e)] : 0.f;
+        [&](bool valid, uint64_t e, uint32_t) { return valid ? ldg(a.col + e) : 0u; },
+        [&](bool valid, uint64_t, uint32_t u, uint32_t) { return valid ? c_in[u] : 0.f; },
+        [&](bool valid, uint32_t owner, uint32_t, uint32_t, float x) {
           if (seg_reduce(valid, owner, x)) s_acc[wib][owner] += x;
           __syncwarp();
         },
@@ -151,7 +153,13 @@ __global__ void __launch_bounds__(kBlock) pr_pull_persistent(PrArgs a) {
         },
         [&](uint32_t v, uint64_t b, uint64_t e) {
           float s = 0.f;
-          for (uint64_t i = b + lane; i < e; i += 32) s += c_in[ldg(a.col + i)];
+          for (uint64_t i = b + lane; i < e; i += 128) {
+            uint32_t u[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) u[k] = i + 32 * k < e ? ldg(a.col + i + 32 * k) : 0xFFFFFFFFu;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) s += u[k] != 0xFFFFFFFFu ? c_in[u[k]] : 0.f;
+          }
           s = warp_sum(s);
           if (lane == 0) atomicAdd(&a.acc[v], s);
         });
