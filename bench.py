@@ -53,12 +53,15 @@ def parse_args():
 
 # ---------------------------------------------------------------- plumbing --
 class Dist:
-    """torch.distributed over NCCL when launched by torchrun, else a no-op."""
+    """torch.distributed when launched by torchrun (WORLD_SIZE > 1), else a
+    no-op.  NCCL on GPUs; `backend="gloo"` keeps everything on the host (the
+    CPU tests of the barrier / max-over-ranks timing use it)."""
 
-    def __init__(self, want_pg: bool):
+    def __init__(self, want_pg: bool, backend: str = "nccl", timeout_s: float = 600.0):
         self.rank = int(os.environ.get("RANK", "0"))
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = False
         if self.world > 1 and want_pg:
             import datetime
@@ -66,9 +69,11 @@ class Dist:
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local_rank))
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(self.local_rank)
+                kw["device_id"] = torch.device("cuda", self.local_rank)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
             self.pg = True
 
     def barrier(self):
@@ -83,7 +88,7 @@ class Dist:
         import torch
         import torch.distributed as dist
 
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -92,6 +97,13 @@ class Dist:
             import torch.distributed as dist
 
             dist.destroy_process_group()
+            self.pg = False
+
+
+def aggregate_rate(world: int, units_per_step: float, steps: int, t_ms_max: float) -> float:
+    """Whole-job throughput in G-units/s: every rank processes units_per_step
+    per step (replicas / weak scaling), timed as the slowest rank."""
+    return world * units_per_step * steps / (t_ms_max / 1e3) / 1e9
 
 
 class ClockSampler:
@@ -650,7 +662,7 @@ def main() -> None:
     dist.barrier()
     clk = clocks.stop()
     t_ms = dist.max(e0.elapsed_time(e1))
-    value = dist.world * units_step * args.steps / (t_ms / 1e3) / 1e9
+    value = aggregate_rate(dist.world, units_step, args.steps, t_ms)
     peak, peak_src = measured_peak_hbm()
     achieved = bytes_step / (sum(kms) / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -718,7 +730,7 @@ def main() -> None:
         for _ in range(ke):
             e2e_step()
         te = dist.max(time.perf_counter() - t0)
-        line["e2e"] = {"value": dist.world * units_step * ke / te / 1e9, "unit": job.unit,
+        line["e2e"] = {"value": aggregate_rate(dist.world, units_step, ke, te * 1e3), "unit": job.unit,
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": ke,
                        "path": "gb_graph_upload (pinned host CSR) + kernel + host output copy + gb_graph_free"}
     for dg in dgs:

@@ -8,6 +8,8 @@ Every .cu under csrc/ is compiled with
 and every .cpp with g++ -O3 -fopenmp; the objects are linked into
 galois_b200/libgb.so against the static CUDA runtime.  Objects live in
 galois_b200/_build/ and are rebuilt when a source or header is newer.
+The command-line programs in apps/ (bfs-gpu, sssp-gpu, cc-gpu, pagerank-gpu,
+bc-gpu, operator-example) are then linked against libgb.so into apps/bin/.
 """
 from __future__ import annotations
 
@@ -24,6 +26,8 @@ CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libgb.so"
 INCLUDE = HERE.parent / "include"
+APPS = HERE / "apps"
+APPS_BIN = APPS / "bin"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -85,7 +89,39 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False) -
         if rc != 0:
             sys.stderr.write(" ".join(cmd) + "\n" + out)
             raise RuntimeError("link of libgb.so failed")
+    build_apps(jobs, force, verbose)
     return LIB
+
+
+def build_apps(jobs: int | None = None, force: bool = False, verbose: bool = False) -> list[Path]:
+    """Link every apps/*.cpp (g++) and apps/*.cu (nvcc, extended lambdas) into
+    apps/bin/<name with '-' for '_'> against libgb.so (rpath $ORIGIN/../..)."""
+    nvcc = _nvcc()
+    APPS_BIN.mkdir(exist_ok=True)
+    headers = _headers() + sorted(APPS.glob("*.h")) + sorted(INCLUDE.glob("*.cuh")) + [LIB]
+    link = [f"-L{HERE}", "-lgb", "-Wl,-rpath,$ORIGIN/../.."]
+    cmds, outs = [], []
+    for src in sorted(APPS.glob("*.cpp")) + sorted(APPS.glob("*.cu")):
+        exe = APPS_BIN / src.stem.replace("_", "-")
+        outs.append(exe)
+        if not (force or _stale(src, exe, headers)):
+            continue
+        if src.suffix == ".cpp":
+            cmds.append(["/usr/bin/g++", "-O2", "-std=c++17", f"-I{INCLUDE}", f"-I{APPS}", str(src),
+                         "-o", str(exe), *link])
+        else:
+            cmds.append([nvcc, *ARCH, "-O2", "-std=c++17", "--extended-lambda", f"-I{INCLUDE}", f"-I{APPS}",
+                         str(src), "-o", str(exe), "-Xlinker", f"-L{HERE},-lgb,-rpath,$ORIGIN/../.."])
+    failed = []
+    with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        for cmd, rc, out in ex.map(_compile, cmds):
+            if verbose or rc != 0:
+                sys.stderr.write(" ".join(cmd) + "\n" + out)
+            if rc != 0:
+                failed.append(cmd[-1] if cmd[0].endswith("g++") else cmd[-3])
+    if failed:
+        raise RuntimeError(f"app build failed: {failed}")
+    return outs
 
 
 def main() -> None:

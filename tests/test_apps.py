@@ -1,0 +1,148 @@
+"""The lonestar-style command-line programs (galois_b200/apps/bin/*-gpu) and
+the operator-layer example.  CPU tests cover the flag surface and error
+paths; GPU tests run each program on a written .gr and compare its report
+lines with the oracle."""
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from galois_b200 import assign_weights_u32, rmat, transpose, write_gr
+
+BIN = Path(__file__).resolve().parents[1] / "galois_b200" / "apps" / "bin"
+APPS = ["bfs-gpu", "sssp-gpu", "cc-gpu", "pagerank-gpu", "bc-gpu", "operator-example"]
+
+
+def run(app, *args, check=True):
+    p = subprocess.run([str(BIN / app), *map(str, args)], capture_output=True, text=True, timeout=300)
+    if check and p.returncode != 0:
+        raise AssertionError(f"{app} exited {p.returncode}\n{p.stdout}\n{p.stderr}")
+    return p
+
+
+def stats(out: str) -> dict:
+    """STAT lines -> {(region, category): value}."""
+    lines = out.splitlines()
+    assert "STAT_TYPE, REGION, CATEGORY, TOTAL_TYPE, TOTAL" in lines
+    d = {}
+    for ln in lines:
+        if ln.startswith("STAT, "):
+            _, region, cat, total_type, val = [x.strip() for x in ln.split(",")]
+            assert total_type == "TMAX"
+            d[(region, cat)] = float(val)
+    return d
+
+
+@pytest.mark.parametrize("app", APPS[:-1])
+def test_app_help(app):
+    p = run(app, "-help")
+    assert p.stdout.startswith(app)
+
+
+@pytest.mark.parametrize("app", APPS)
+def test_app_missing_file(app, tmp_path):
+    p = run(app, tmp_path / "absent.gr", check=False)
+    assert p.returncode == 1
+    assert "ERROR" in p.stderr
+
+
+def test_app_flag_contracts(tmp_path):
+    # cc needs -symmetricGraph, pull PageRank needs -transposedGraph (as the reference apps)
+    p = run("cc-gpu", tmp_path / "x.gr", check=False)
+    assert p.returncode == 1 and "symmetric" in p.stderr
+    p = run("pagerank-gpu", tmp_path / "x.gr", check=False)
+    assert p.returncode == 1 and "transposed" in p.stderr
+
+
+# ---- GPU --------------------------------------------------------------------------
+
+
+@pytest.fixture(scope="module")
+def graphs(tmp_path_factory):
+    d = tmp_path_factory.mktemp("apps")
+    g, perm = rmat(12, 8, seed=5)
+    g = assign_weights_u32(g, 1, 100, seed=3)
+    write_gr(str(d / "g.gr"), g, 4)
+    gt, _ = transpose(g)
+    write_gr(str(d / "gt.gr"), gt, 0)
+    return d, g, gt, int(perm[0])
+
+
+def _node_line(out, report):
+    m = re.search(rf"Node {report} has distance (\d+)", out)
+    assert m, out
+    return int(m.group(1))
+
+
+@pytest.mark.gpu
+def test_bfs_gpu_app(cuda_device, graphs):
+    d, g, _, src = graphs
+    report = int(np.argmax(g.degrees()))
+    p = run("bfs-gpu", d / "g.gr", f"-startNode={src}", "-reportNode", report, "-symmetricGraph")
+    want = oracle.bfs_serial(g, src)
+    assert _node_line(p.stdout, report) == int(want[report])
+    assert f"# visited nodes is {int((want != oracle.INF).sum())}" in p.stdout
+    assert "Verification successful." in p.stdout
+    st = stats(p.stdout)
+    assert st[("BFS", "Rounds")] >= 1
+
+
+@pytest.mark.gpu
+def test_sssp_gpu_app(cuda_device, graphs, tmp_path):
+    d, g, _, src = graphs
+    p = run("sssp-gpu", d / "g.gr", f"-startNode={src}", "-reportNode=7", "-delta=4",
+            f"-statFile={tmp_path / 'st.txt'}")
+    want = oracle.sssp_dijkstra(g, src)
+    assert _node_line(p.stdout, 7) == int(want[7])
+    reached = want != oracle.INF
+    assert f"Sum of visited distances is {int(want[reached].astype(np.uint64).sum())}" in p.stdout
+    assert "Verification successful." in p.stdout
+    st = stats((tmp_path / "st.txt").read_text())
+    assert st[("SSSP", "Buckets")] >= 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algo", ["LabelProp", "Afforest", "EdgetiledAsync"])
+def test_cc_gpu_app(cuda_device, graphs, algo):
+    d, g, _, _ = graphs
+    p = run("cc-gpu", d / "g.gr", "-symmetricGraph", f"-algo={algo}")
+    lab = oracle.cc_union_find(g)
+    assert f"Total components: {len(np.unique(lab))}" in p.stdout
+    assert "Verification successful." in p.stdout
+
+
+@pytest.mark.gpu
+def test_pagerank_gpu_app(cuda_device, graphs):
+    d, _, gt, _ = graphs
+    p = run("pagerank-gpu", d / "gt.gr", "-transposedGraph", "-tolerance=1e-6")
+    want, _ = oracle.pr_pull_topo_f64(gt, 0.85, 1e-6, 1000)
+    top = [ln.split() for ln in p.stdout.split("Rank PageRank Id\n")[1].splitlines()[:5]]
+    for _, val, vid in top:
+        assert abs(float(val) - want[int(vid)]) <= 1e-5
+    assert int(top[0][2]) == int(np.argmax(want))
+    assert stats(p.stdout)[("PageRank", "Iterations")] >= 1
+
+
+@pytest.mark.gpu
+def test_bc_gpu_app(cuda_device, graphs, tmp_path):
+    d, g, _, _ = graphs
+    srcs = [int(x) for x in np.argsort(-g.degrees(), kind="stable")[:40]]
+    (tmp_path / "srcs.txt").write_text(" ".join(map(str, srcs)))
+    p = run("bc-gpu", d / "g.gr", f"-sourcesToUse={tmp_path / 'srcs.txt'}", "-numOfSources=40", "-output")
+    want = oracle.bc_level(g, srcs, f64=True)
+    got = np.zeros(g.n)
+    for ln in p.stdout.splitlines():
+        parts = ln.split()
+        if len(parts) == 2 and parts[0].isdigit():
+            got[int(parts[0])] = float(parts[1])
+    assert np.max(np.abs(got - want)) <= 1e-4 * max(1.0, float(np.max(want)))
+
+
+@pytest.mark.gpu
+def test_operator_example(cuda_device, graphs):
+    d, _, _, src = graphs
+    p = run("operator-example", d / "g.gr", f"-startNode={src}")
+    assert "0 mismatches" in p.stdout and "Verification successful." in p.stdout
