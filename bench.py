@@ -40,8 +40,12 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--app", choices=["sssp", "bfs", "cc", "pr", "bc", "multigraph", "ppr"], default="sssp")
-    ap.add_argument("--size", choices=["small", "medium", "full"], default="full",
-                    help="graph sizes: full = the benchmark configuration; medium/small for profiling")
+    ap.add_argument("--size", choices=["small", "medium", "full", "s24"], default="full",
+                    help="graph sizes: full = the benchmark configuration; s24 = RMAT scale 24 for every "
+                         "app; medium/small for profiling")
+    ap.add_argument("--order", type=int, choices=[0, 1, 2], default=1,
+                    help="vertex order of the resident graph: 0 file order, 1 degree-ordered with sorted "
+                         "rows (gb_graph_reorder, done once before timing), 2 degree-ordered unsorted rows")
     ap.add_argument("--small", action="store_true", help="same as --size small")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -185,8 +189,8 @@ def pinned_copy(a: np.ndarray) -> np.ndarray:
 _PINNED: list = []
 
 
-def pick(size: str, small, medium, full):
-    return {"small": small, "medium": medium, "full": full}[size]
+def pick(size: str, small, medium, full, s24=None):
+    return {"small": small, "medium": medium, "full": full, "s24": full if s24 is None else s24}[size]
 
 
 def emit(line: dict) -> None:
@@ -243,7 +247,8 @@ class SsspJob(Job):
         super().__init__(size)
         from galois_b200 import assign_weights_u32, grid2d, rmat
 
-        scale, side = pick(size, (16, 512), (20, 2048), (22, 4096))
+        scale, side = pick(size, (16, 512), (20, 2048), (22, 4096), (24, 4096))
+        self.workload = self.workload.replace("RMAT-22", f"RMAT-{scale}")
         g, perm = rmat(scale, 16, seed=22, symmetrize=False)
         assign_weights_u32(g, 1, 255, seed=22)
         self.graphs.append({"name": f"rmat{scale}-directed", "host": g, "symmetric": False, "src": int(perm[0])})
@@ -276,7 +281,8 @@ class BfsJob(Job):
         super().__init__(size)
         from galois_b200 import rmat
 
-        scale = pick(size, 16, 18, 20)
+        scale = pick(size, 16, 18, 20, 24)
+        self.workload = self.workload.replace("RMAT-20", f"RMAT-{scale}")
         g, _ = rmat(scale, 16, seed=20, symmetrize=True)
         self.graphs.append({"name": f"rmat{scale}-sym", "host": g, "symmetric": True,
                             "src": int(np.argmax(g.degrees()))})
@@ -371,6 +377,8 @@ class PrJob(Job):
 
 
 JOBS = {"sssp": SsspJob, "bfs": BfsJob, "cc": CcJob, "pr": PrJob}
+ORDER_NAMES = {0: "file order", 1: "degree-ordered (gb_graph_reorder, sorted rows)",
+               2: "degree-ordered (gb_graph_reorder, unsorted rows)"}
 BATCHED = ("bc", "multigraph", "ppr")
 
 
@@ -634,9 +642,15 @@ def main() -> None:
     torch.cuda.set_device(dev)
     job = job_cls(args.size)
     tname, npdt = job.out_kind()
-    dgs, outs = [], []
+    dgs, outs, reorder_ms = [], [], []
     for g in job.graphs:
-        dgs.append(DeviceGraph(g["host"], symmetric=g["symmetric"], device=dev))
+        dg = DeviceGraph(g["host"], symmetric=g["symmetric"], device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if args.order:
+            dg.reorder(args.order)  # graph preparation, once, outside the timed region
+        reorder_ms.append((time.perf_counter() - t0) * 1e3)
+        dgs.append(dg)
         outs.append(torch.empty(g["host"].n, dtype=getattr(torch, tname), device=f"cuda:{dev}"))
     # stats runs: warm the workspaces, collect units, bytes and kernel time
     st_runs = [[job.stats_call(dg, gi, outs[gi]) for gi, dg in enumerate(dgs)] for _ in range(3)]
@@ -672,8 +686,9 @@ def main() -> None:
     line = {"metric": job.metric, "value": value, "unit": job.unit, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": job.dtype, "data": "synthetic (seeded generators)",
-            "config": job.config(), "roofline": roofline, "clocks": clk,
-            "gpu_launches": 2 * len(dgs) * args.steps,
+            "config": {**job.config(), "vertex_order": ORDER_NAMES[args.order]}, "roofline": roofline, "clocks": clk,
+            "gpu_launches": sum(int(st["launches"]) for st in stats) * args.steps,
+            "reorder_ms": reorder_ms,
             "detail": [{"graph": job.graphs[gi]["name"], **{k: stats[gi][k] for k in stats[gi]}}
                        for gi in range(len(dgs))]}
     # ---- CPU baseline (rank 0, one GPU only) -----------------------------------
@@ -732,7 +747,8 @@ def main() -> None:
         te = dist.max(time.perf_counter() - t0)
         line["e2e"] = {"value": aggregate_rate(dist.world, units_step, ke, te * 1e3), "unit": job.unit,
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": ke,
-                       "path": "gb_graph_upload (pinned host CSR) + kernel + host output copy + gb_graph_free"}
+                       "path": "gb_graph_upload (pinned host CSR, file order: a one-shot call does not "
+                               "amortise gb_graph_reorder) + kernel + host output copy + gb_graph_free"}
     for dg in dgs:
         dg.free()
     if dist.rank == 0:

@@ -26,6 +26,9 @@ GB_DIST_INFINITY = 2147483646
 GB_CC_LABELPROP = 0
 GB_CC_UNIONFIND = 1
 GB_CC_AFFOREST = 2
+GB_ORDER_NONE = 0
+GB_ORDER_DEGREE = 1
+GB_ORDER_DEGREE_UNSORTED = 2
 
 _STATUS_NAMES = {
     GB_ERR_ARG: "GB_ERR_ARG", GB_ERR_OOM: "GB_ERR_OOM", GB_ERR_CUDA: "GB_ERR_CUDA",
@@ -109,6 +112,8 @@ SIGNATURES: dict[str, tuple] = {
     "gb_graph_device_arrays": (C.c_int, [_gp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
                                          C.POINTER(_vp)]),
     "gb_graph_build_transpose": (C.c_int, [_gp, _vp]),
+    "gb_graph_reorder": (C.c_int, [_gp, C.c_int, _vp]),
+    "gb_graph_permutation": (C.c_int, [_gp, C.POINTER(_vp), C.POINTER(_vp)]),
     "gb_graph_set_tuning": (C.c_int, [_gp, C.POINTER(Tuning)]),
     "gb_graph_get_tuning": (C.c_int, [_gp, C.POINTER(Tuning)]),
     "gb_bfs": (C.c_int, [_gp, C.c_uint32, _vp, C.POINTER(Stats), _vp]),

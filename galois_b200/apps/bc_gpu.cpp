@@ -3,7 +3,7 @@
 // (LevelStructs.h:253-297): -sourcesToUse=<file of ids>, else 0..numOfSources-1
 // (-numOfSources=0 means every vertex), or just -startNode with
 // -singleSource.  -batch sets the sources per multi-source launch (1..64,
-// default 64).  Sanity lines and -output as LevelStructs.h:195-217, 314-323.
+// default 64; batches need -symmetricGraph, else one source per launch).  Sanity lines and -output as LevelStructs.h:195-217, 314-323.
 #include <algorithm>
 #include <fstream>
 #include <iterator>
@@ -44,7 +44,12 @@ int main(int argc, char** argv) {
   }
   for (uint32_t s : srcs)
     if (s >= n) die("source " + std::to_string(s) + " is not a vertex");
-  const uint32_t batch = (uint32_t)f.u64("batch", 64);
+  uint32_t batch = (uint32_t)f.u64("batch", 64);
+  if (batch > 1 && !f.flag("symmetricGraph")) {
+    // the multi-source kernels pull over in-edges, which only a symmetric graph has without a transpose
+    info("multi-source batches need -symmetricGraph; running one source per launch");
+    batch = 1;
+  }
   info("Running level BC on the GPU with " + std::to_string(srcs.size()) + " sources, batch " +
        std::to_string(batch));
   std::vector<float> bc(n);

@@ -94,6 +94,7 @@ extern "C" int gb_autotune(gb_graph* g, const char* kernel, uint32_t src, const 
     GB_FAIL(GB_ERR_ARG, "gb_autotune: kernel must be bfs, sssp, cc or pr");
   if ((k == "bfs" || k == "sssp") && src >= g->n) GB_FAIL(GB_ERR_ARG, "gb_autotune: source %u >= n", src);
   if (k == "sssp" && !g->w) GB_FAIL(GB_ERR_ARG, "gb_autotune: sssp needs uint32 weights");
+  if (g->perm && (k == "bfs" || k == "sssp")) src = g->h_iperm[src];  // relabelled graph: internal id
   GB_CUDA(cudaSetDevice(g->device));
   const std::string cls = graph_class(g);
   gb_tuning cached{};

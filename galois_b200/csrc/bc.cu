@@ -682,5 +682,18 @@ extern "C" int gb_bc(gb_graph* g, const uint32_t* srcs, uint32_t nsrc, uint32_t 
   gb::clear_error();
   if (!g || !bc_out || (nsrc && !srcs)) GB_FAIL(GB_ERR_ARG, "gb_bc: null argument");
   GB_CUDA(cudaSetDevice(g->device));
-  return gb::run_bc(g, srcs, nsrc, batch, bc_out, stats, static_cast<cudaStream_t>(stream));
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (g->perm) {
+    std::vector<uint32_t> mapped(nsrc);
+    for (uint32_t i = 0; i < nsrc; ++i) {
+      if (srcs[i] >= g->n) GB_FAIL(GB_ERR_ARG, "gb_bc: source %u >= n %u", srcs[i], g->n);
+      mapped[i] = g->h_iperm[srcs[i]];
+    }
+    float* res = reinterpret_cast<float*>(gb::result_buf(g, 0));
+    int st = gb::run_bc(g, mapped.data(), nsrc, batch, res, stats, s);
+    if (st != GB_OK) return st;
+    if (stats) stats->launches += 1;  // the mapping gather
+    return gb::finish_f32(g, res, bc_out, s);
+  }
+  return gb::run_bc(g, srcs, nsrc, batch, bc_out, stats, s);
 }

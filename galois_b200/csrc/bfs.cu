@@ -393,7 +393,19 @@ extern "C" int gb_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* 
   if (!g || !level_out) GB_FAIL(GB_ERR_ARG, "gb_bfs: null argument");
   if (src >= g->n) GB_FAIL(GB_ERR_ARG, "gb_bfs: source %u >= n %u", src, g->n);
   GB_CUDA(cudaSetDevice(g->device));
-  return gb::run_bfs(g, src, level_out, stats, static_cast<cudaStream_t>(stream), nullptr, 0);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (g->perm) {
+    // relabelled graph: run on internal ids, map the levels back (a stats
+    // struct makes run_bfs check the device status before host copies)
+    gb_stats local{};
+    uint32_t* res = gb::result_buf(g, 0);
+    int st = gb::run_bfs(g, g->h_iperm[src], res, stats ? stats : (gb::is_device_ptr(level_out) ? nullptr : &local),
+                         s, nullptr, 0);
+    if (st != GB_OK) return st;
+    if (stats) stats->launches += 1;  // the mapping gather
+    return gb::finish_u32(g, res, level_out, s);
+  }
+  return gb::run_bfs(g, src, level_out, stats, s, nullptr, 0);
 }
 
 // ---------------------------------------------------------------------------

@@ -304,5 +304,16 @@ extern "C" int gb_cc(gb_graph* g, int algo, uint32_t* label_out, gb_stats* stats
   gb::clear_error();
   if (!g || !label_out) GB_FAIL(GB_ERR_ARG, "gb_cc: null argument");
   GB_CUDA(cudaSetDevice(g->device));
-  return gb::run_cc(g, algo, label_out, stats, static_cast<cudaStream_t>(stream));
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (g->perm) {
+    // labels come back as min internal ids; finish_labels makes them the
+    // min ORIGINAL id of each component
+    gb_stats local{};
+    uint32_t* res = gb::result_buf(g, 0);
+    int st = gb::run_cc(g, algo, res, stats ? stats : (gb::is_device_ptr(label_out) ? nullptr : &local), s);
+    if (st != GB_OK) return st;
+    if (stats) stats->launches += 2;  // component minimum + mapping
+    return gb::finish_labels(g, res, label_out, s);
+  }
+  return gb::run_cc(g, algo, label_out, stats, s);
 }

@@ -54,6 +54,15 @@ struct gb_graph {
   // personalised-PageRank state (opaque, owned by ppr.cu)
   void* ppr_state = nullptr;
   void (*ppr_free)(gb_graph*) = nullptr;
+  // degree-ordered relabelling (reorder.cu): when perm is set, every array
+  // above uses internal ids; perm[new] = original id, iperm[original] = new
+  // id (device), h_iperm the host copy for mapping sources; ro_buf holds 3n
+  // words of result staging for mapping outputs back to original ids
+  int order = 0;
+  uint32_t* perm = nullptr;
+  uint32_t* iperm = nullptr;
+  uint32_t* h_iperm = nullptr;
+  uint32_t* ro_buf = nullptr;
   // scratch workspace, grown on demand
   void* ws = nullptr;
   size_t ws_bytes = 0;
@@ -109,6 +118,16 @@ int copy_out(void* dst, const void* src_dev, size_t bytes, cudaStream_t stream);
 int copy_in(void* dst_dev, const void* src, size_t bytes, cudaStream_t stream);
 
 int ensure_transpose(gb_graph* g, cudaStream_t stream);
+
+// Relabelled graphs (reorder.cu).  result_buf returns the k-th n-word
+// staging buffer (k < 3).  finish_* map a result computed in internal ids
+// (device, in result_buf(g, 0)) to original ids in `out` (host or device);
+// finish_labels also turns min-internal-id labels into min-original-id labels.
+uint32_t* result_buf(gb_graph* g, int k);
+int reserve_result_bufs(gb_graph* g);
+int finish_u32(gb_graph* g, const uint32_t* res, uint32_t* out, cudaStream_t s);
+int finish_f32(gb_graph* g, const float* res, float* out, cudaStream_t s);
+int finish_labels(gb_graph* g, const uint32_t* res, uint32_t* out, cudaStream_t s);
 
 // Times one kernel launch with CUDA events on its stream (only when `on`).
 struct KernelTimer {

@@ -8,6 +8,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "device_common.cuh"
@@ -326,6 +327,10 @@ int gb_graph_free(gb_graph* g) {
   cudaFree(g->mg_level);
   cudaFree(g->mg_label);
   if (g->mg_stage) cudaFreeHost(g->mg_stage);
+  cudaFree(g->perm);
+  cudaFree(g->iperm);
+  cudaFree(g->ro_buf);
+  std::free(g->h_iperm);
   cudaFree(g->ws);
   if (g->pinned) cudaFreeHost(g->pinned);
   delete g;

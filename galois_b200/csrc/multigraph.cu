@@ -116,6 +116,7 @@ extern "C" int gb_multi_graph_bfs_cc(gb_graph* g, const uint32_t* graph_first, u
     GB_FAIL(GB_ERR_ARG, "gb_multi_graph_bfs_cc: null argument");
   if (ngraphs == 0 || ngraphs > g->n) GB_FAIL(GB_ERR_ARG, "gb_multi_graph_bfs_cc: bad graph count %u", ngraphs);
   if (!g->symmetric) GB_FAIL(GB_ERR_UNSUPPORTED, "gb_multi_graph_bfs_cc: needs symmetric graphs");
+  if (g->perm) GB_FAIL(GB_ERR_UNSUPPORTED, "gb_multi_graph_bfs_cc: the block-diagonal layout needs file order (graph was relabelled)");
   if (is_device_ptr(graph_first) || is_device_ptr(local_src))
     GB_FAIL(GB_ERR_ARG, "gb_multi_graph_bfs_cc: graph_first and local_src are host arrays");
   GB_CUDA(cudaSetDevice(g->device));

@@ -498,6 +498,22 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
 
 }  // namespace
 
+// Entry wrapper: on a relabelled graph the ranks are computed in internal ids
+// and mapped back (also when the iteration cap was hit: the ranks are set).
+int pagerank_entry(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_iter, float* rank_out,
+                   uint32_t* iters_out, gb_stats* stats, cudaStream_t s, float init = -1.f, float base = -1.f,
+                   int linf = 0) {
+  if (!g->perm) return run_pagerank(g, kind, alpha, tol, max_iter, rank_out, iters_out, stats, s, init, base, linf);
+  gb_stats local{};
+  float* res = reinterpret_cast<float*>(result_buf(g, 0));
+  int st = run_pagerank(g, kind, alpha, tol, max_iter, res, iters_out,
+                        stats ? stats : (is_device_ptr(rank_out) ? nullptr : &local), s, init, base, linf);
+  if (st != GB_OK && st != GB_ERR_NOT_CONVERGED) return st;
+  if (stats) stats->launches += 1;  // the mapping gather
+  const int fs = finish_f32(g, res, rank_out, s);
+  return fs != GB_OK ? fs : st;
+}
+
 }  // namespace gb
 
 extern "C" {
@@ -507,8 +523,8 @@ int gb_pagerank_pull(gb_graph* g, float alpha, float tol, uint32_t max_iter, flo
   gb::clear_error();
   if (!g || !rank_out) GB_FAIL(GB_ERR_ARG, "gb_pagerank_pull: null argument");
   GB_CUDA(cudaSetDevice(g->device));
-  return gb::run_pagerank(g, gb::PrKind::Pull, alpha, tol, max_iter, rank_out, iters_out, stats,
-                          static_cast<cudaStream_t>(stream));
+  return gb::pagerank_entry(g, gb::PrKind::Pull, alpha, tol, max_iter, rank_out, iters_out, stats,
+                            static_cast<cudaStream_t>(stream));
 }
 
 int gb_pagerank_pull_ex(gb_graph* g, float alpha, float tol, uint32_t max_iter, float init, float base,
@@ -517,8 +533,8 @@ int gb_pagerank_pull_ex(gb_graph* g, float alpha, float tol, uint32_t max_iter, 
   if (!g || !rank_out) GB_FAIL(GB_ERR_ARG, "gb_pagerank_pull_ex: null argument");
   if (!(init >= 0.f) || !(base >= 0.f)) GB_FAIL(GB_ERR_ARG, "gb_pagerank_pull_ex: init and base must be >= 0");
   GB_CUDA(cudaSetDevice(g->device));
-  return gb::run_pagerank(g, gb::PrKind::Pull, alpha, tol, max_iter, rank_out, iters_out, stats,
-                          static_cast<cudaStream_t>(stream), init, base, norm_linf ? 1 : 0);
+  return gb::pagerank_entry(g, gb::PrKind::Pull, alpha, tol, max_iter, rank_out, iters_out, stats,
+                            static_cast<cudaStream_t>(stream), init, base, norm_linf ? 1 : 0);
 }
 
 int gb_pagerank_pull_residual(gb_graph* g, float alpha, float tol, uint32_t max_iter, float* rank_out,
@@ -526,8 +542,8 @@ int gb_pagerank_pull_residual(gb_graph* g, float alpha, float tol, uint32_t max_
   gb::clear_error();
   if (!g || !rank_out) GB_FAIL(GB_ERR_ARG, "gb_pagerank_pull_residual: null argument");
   GB_CUDA(cudaSetDevice(g->device));
-  return gb::run_pagerank(g, gb::PrKind::PullResidual, alpha, tol, max_iter, rank_out, iters_out, stats,
-                          static_cast<cudaStream_t>(stream));
+  return gb::pagerank_entry(g, gb::PrKind::PullResidual, alpha, tol, max_iter, rank_out, iters_out, stats,
+                            static_cast<cudaStream_t>(stream));
 }
 
 int gb_pagerank_push(gb_graph* g, float alpha, float tol, uint32_t max_iter, float* rank_out,
@@ -535,8 +551,8 @@ int gb_pagerank_push(gb_graph* g, float alpha, float tol, uint32_t max_iter, flo
   gb::clear_error();
   if (!g || !rank_out) GB_FAIL(GB_ERR_ARG, "gb_pagerank_push: null argument");
   GB_CUDA(cudaSetDevice(g->device));
-  return gb::run_pagerank(g, gb::PrKind::Push, alpha, tol, max_iter, rank_out, iters_out, stats,
-                          static_cast<cudaStream_t>(stream));
+  return gb::pagerank_entry(g, gb::PrKind::Push, alpha, tol, max_iter, rank_out, iters_out, stats,
+                            static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

@@ -450,6 +450,8 @@ int solve(gb_graph* g, PprState* st, bool adjoint, uint32_t B, const float* src,
 }
 
 int check_common(gb_graph* g, uint32_t B, float alpha, uint32_t max_iter) {
+  // teleport / rank / arc-weight arrays are indexed by the caller's ids and arcs
+  if (g->perm) GB_FAIL(GB_ERR_UNSUPPORTED, "ppr: graph was relabelled; PPR needs file order");
   if (!(B == 1 || (B % 4 == 0 && B >= 4 && B <= 128))) GB_FAIL(GB_ERR_ARG, "ppr: B must be 1 or a multiple of 4 <= 128");
   if (!(alpha > 0.f && alpha < 1.f)) GB_FAIL(GB_ERR_ARG, "ppr: alpha must be in (0,1)");
   if (max_iter == 0) GB_FAIL(GB_ERR_ARG, "ppr: max_iter must be > 0");

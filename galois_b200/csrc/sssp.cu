@@ -408,5 +408,15 @@ extern "C" int gb_sssp_delta(gb_graph* g, uint32_t src, uint32_t delta_shift, ui
   if (!g || !dist_out) GB_FAIL(GB_ERR_ARG, "gb_sssp_delta: null argument");
   if (src >= g->n) GB_FAIL(GB_ERR_ARG, "gb_sssp_delta: source %u >= n %u", src, g->n);
   GB_CUDA(cudaSetDevice(g->device));
-  return gb::run_sssp(g, src, delta_shift, dist_out, stats, static_cast<cudaStream_t>(stream));
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (g->perm) {
+    gb_stats local{};
+    uint32_t* res = gb::result_buf(g, 0);
+    int st = gb::run_sssp(g, g->h_iperm[src], delta_shift, res,
+                          stats ? stats : (gb::is_device_ptr(dist_out) ? nullptr : &local), s);
+    if (st != GB_OK) return st;
+    if (stats) stats->launches += 1;  // the mapping gather
+    return gb::finish_u32(g, res, dist_out, s);
+  }
+  return gb::run_sssp(g, src, delta_shift, dist_out, stats, s);
 }

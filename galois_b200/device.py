@@ -49,7 +49,10 @@ def _buf(x, count: int, np_dtype, what: str):
 class DeviceGraph:
     """Device-resident CSR (gb_graph*)."""
 
-    def __init__(self, g: HostCSR, symmetric: bool = False, device: int = 0):
+    def __init__(self, g: HostCSR, symmetric: bool = False, device: int = 0, reorder: int = 0):
+        """reorder: 0 keeps file order, 1 (GB_ORDER_DEGREE) relabels by
+        descending degree with sorted rows, 2 without the row sort.  Results
+        are in original ids either way."""
         handle = C.c_void_p()
         wu = C.c_void_p(g.w_u32.ctypes.data) if g.w_u32 is not None else None
         wf = C.c_void_p(g.w_f32.ctypes.data) if g.w_f32 is not None else None
@@ -60,6 +63,17 @@ class DeviceGraph:
         self.m = g.m
         self.symmetric = bool(symmetric)
         self.device = device
+        if reorder:
+            self.reorder(reorder)
+
+    def reorder(self, order: int = _lib.GB_ORDER_DEGREE) -> None:
+        check(lib.gb_graph_reorder(self.handle, int(order), None), "gb_graph_reorder")
+
+    def permutation(self) -> dict:
+        """Device pointers of the relabelling (None when in file order)."""
+        p = [C.c_void_p() for _ in range(2)]
+        check(lib.gb_graph_permutation(self.handle, *[C.byref(x) for x in p]), "gb_graph_permutation")
+        return {"new_to_old": p[0].value, "old_to_new": p[1].value}
 
     @classmethod
     def from_handle(cls, handle: C.c_void_p) -> "DeviceGraph":
@@ -73,12 +87,15 @@ class DeviceGraph:
         return self
 
     @classmethod
-    def load_gr(cls, path: str, edge_bytes: int = 0, symmetric: bool = False, device: int = 0) -> "DeviceGraph":
+    def load_gr(cls, path: str, edge_bytes: int = 0, symmetric: bool = False, device: int = 0,
+                reorder: int = 0) -> "DeviceGraph":
         h = C.c_void_p()
         check(lib.gb_graph_load_gr(str(path).encode(), edge_bytes, int(symmetric), device, C.byref(h)),
               "gb_graph_load_gr")
         g = cls.from_handle(h)
         g.device = device
+        if reorder:
+            g.reorder(reorder)
         return g
 
     @property

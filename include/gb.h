@@ -149,6 +149,27 @@ int gb_graph_device_arrays(const gb_graph* g, const uint64_t** offs,
  * directed graphs and for the PPR forward pass. */
 int gb_graph_build_transpose(gb_graph* g, void* stream);
 
+/* Degree-ordered relabelling of the device mirror (no counterpart in the
+ * reference, which keeps file order).  GB_ORDER_DEGREE renumbers vertices by
+ * descending out-degree (ties by id) and sorts each adjacency list (when
+ * m < 2^31; larger graphs keep the relabelled file order), so that the
+ * gathers of high-degree vertices share cache lines.  GB_ORDER_DEGREE_UNSORTED
+ * skips the row sort.  Every algorithm call keeps taking and returning
+ * ORIGINAL vertex ids (sources are mapped in, results mapped out; CC labels
+ * stay the minimum original id of the component), so results are unchanged;
+ * gb_graph_device_arrays and gb_graph_build_transpose then describe the
+ * relabelled graph.  Cannot be undone; GB_ORDER_NONE is accepted only on a
+ * graph that was never reordered.  Multi-graph and PPR calls return
+ * GB_ERR_UNSUPPORTED on a reordered graph. */
+#define GB_ORDER_NONE 0
+#define GB_ORDER_DEGREE 1
+#define GB_ORDER_DEGREE_UNSORTED 2
+int gb_graph_reorder(gb_graph* g, int order, void* stream);
+/* Device permutation of a reordered graph: new_to_old[internal id] =
+ * original id, old_to_new the inverse; both NULL if not reordered. */
+int gb_graph_permutation(const gb_graph* g, const uint32_t** new_to_old,
+                         const uint32_t** old_to_new);
+
 /* Per-call statistics (all optional). */
 typedef struct gb_stats {
   uint64_t vertices_reached; /* n_r                                          */

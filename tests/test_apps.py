@@ -78,10 +78,12 @@ def _node_line(out, report):
 
 
 @pytest.mark.gpu
-def test_bfs_gpu_app(cuda_device, graphs):
+@pytest.mark.parametrize("reorder", [0, 1])
+def test_bfs_gpu_app(cuda_device, graphs, reorder):
     d, g, _, src = graphs
     report = int(np.argmax(g.degrees()))
-    p = run("bfs-gpu", d / "g.gr", f"-startNode={src}", "-reportNode", report, "-symmetricGraph")
+    p = run("bfs-gpu", d / "g.gr", f"-startNode={src}", "-reportNode", report, "-symmetricGraph",
+            f"-reorder={reorder}")
     want = oracle.bfs_serial(g, src)
     assert _node_line(p.stdout, report) == int(want[report])
     assert f"# visited nodes is {int((want != oracle.INF).sum())}" in p.stdout
@@ -105,10 +107,11 @@ def test_sssp_gpu_app(cuda_device, graphs, tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("algo", ["LabelProp", "Afforest", "EdgetiledAsync"])
-def test_cc_gpu_app(cuda_device, graphs, algo):
+@pytest.mark.parametrize("algo,reorder", [("LabelProp", 0), ("Afforest", 0), ("EdgetiledAsync", 0),
+                                          ("LabelProp", 1), ("Afforest", 2)])
+def test_cc_gpu_app(cuda_device, graphs, algo, reorder):
     d, g, _, _ = graphs
-    p = run("cc-gpu", d / "g.gr", "-symmetricGraph", f"-algo={algo}")
+    p = run("cc-gpu", d / "g.gr", "-symmetricGraph", f"-algo={algo}", f"-reorder={reorder}")
     lab = oracle.cc_union_find(g)
     assert f"Total components: {len(np.unique(lab))}" in p.stdout
     assert "Verification successful." in p.stdout
@@ -131,7 +134,8 @@ def test_bc_gpu_app(cuda_device, graphs, tmp_path):
     d, g, _, _ = graphs
     srcs = [int(x) for x in np.argsort(-g.degrees(), kind="stable")[:40]]
     (tmp_path / "srcs.txt").write_text(" ".join(map(str, srcs)))
-    p = run("bc-gpu", d / "g.gr", f"-sourcesToUse={tmp_path / 'srcs.txt'}", "-numOfSources=40", "-output")
+    p = run("bc-gpu", d / "g.gr", f"-sourcesToUse={tmp_path / 'srcs.txt'}", "-numOfSources=40", "-output",
+            "-symmetricGraph")
     want = oracle.bc_level(g, srcs, f64=True)
     got = np.zeros(g.n)
     for ln in p.stdout.splitlines():

@@ -1,0 +1,167 @@
+"""Degree-ordered relabelling (gb_graph_reorder): every algorithm keeps taking
+and returning original vertex ids, so the results match the oracle exactly
+(BFS/SSSP/CC) or within the stated tolerance (PageRank, BC), for host and
+device outputs, sorted and unsorted rows, symmetric and directed graphs."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from galois_b200 import (GB_CC_AFFOREST, GB_CC_LABELPROP, GB_CC_UNIONFIND, GB_ORDER_DEGREE,
+                         GB_ORDER_DEGREE_UNSORTED, GB_ORDER_NONE, DeviceGraph, GbError, HostCSR,
+                         assign_weights_f32, assign_weights_u32, grid2d, rmat)
+from galois_b200 import _lib
+from galois_b200.graph import pack_graphs
+
+pytestmark = pytest.mark.gpu
+INF = oracle.INF
+ORDERS = [GB_ORDER_DEGREE, GB_ORDER_DEGREE_UNSORTED]
+
+
+def _dev(n, dtype=torch.int32):
+    return torch.full((n,), -7, dtype=dtype, device="cuda")
+
+
+@pytest.mark.parametrize("order", ORDERS)
+def test_bfs_reordered(cuda_device, order):
+    g, perm = rmat(14, 16, seed=31)
+    deg = g.degrees()
+    srcs = [int(np.argmax(deg)), int(perm[5]), int(np.flatnonzero(deg == 0)[0]) if (deg == 0).any() else 3]
+    with DeviceGraph(g, symmetric=True, reorder=order) as dg:
+        for src in srcs:
+            want = oracle.bfs_serial(g, src)
+            assert (dg.bfs(src) == want).all()
+            out = _dev(g.n)
+            dg.bfs(src, out=out)
+            assert (out.cpu().numpy().view(np.uint32) == want).all()
+        dg.set_tuning(direction_opt=2)
+        assert (dg.bfs(srcs[0]) == oracle.bfs_serial(g, srcs[0])).all()
+
+
+@pytest.mark.parametrize("order", ORDERS)
+def test_sssp_reordered_directed(cuda_device, order):
+    g, perm = rmat(14, 8, seed=32, symmetrize=False)
+    assign_weights_u32(g, 1, 255, seed=5)
+    src = int(perm[0])
+    want = oracle.sssp_dijkstra(g, src)
+    with DeviceGraph(g, reorder=order) as dg:
+        got, st = dg.sssp(src, 13, stats=True)
+        assert (got == want).all()
+        assert st["vertices_reached"] == int((want != INF).sum())
+        out = _dev(g.n)
+        dg.sssp(src, 4, out=out)
+        assert (out.cpu().numpy().view(np.uint32) == want).all()
+
+
+def test_sssp_reordered_grid(cuda_device):
+    g = grid2d(64, 80)
+    assign_weights_u32(g, 1, 255, seed=9)
+    want = oracle.sssp_dijkstra(g, 77)
+    with DeviceGraph(g, symmetric=True, reorder=GB_ORDER_DEGREE) as dg:
+        assert (dg.sssp(77, 6) == want).all()
+
+
+@pytest.mark.parametrize("algo", [GB_CC_LABELPROP, GB_CC_UNIONFIND, GB_CC_AFFOREST])
+@pytest.mark.parametrize("order", ORDERS)
+def test_cc_reordered_min_original_label(cuda_device, algo, order):
+    # RMAT plus a few isolated / small pieces: labels must be the min ORIGINAL id
+    g, _ = rmat(13, 4, seed=33)
+    want = oracle.cc_union_find(g)
+    with DeviceGraph(g, symmetric=True, reorder=order) as dg:
+        assert (dg.cc(algo) == want).all()
+        out = _dev(g.n)
+        dg.cc(algo, out=out)
+        assert (out.cpu().numpy().view(np.uint32) == want).all()
+
+
+@pytest.mark.parametrize("order", ORDERS)
+def test_pagerank_reordered(cuda_device, order):
+    g, _ = rmat(13, 16, seed=34)
+    want, _ = oracle.pr_pull_topo_f64(g, 0.85, 1e-6, 1000)
+    with DeviceGraph(g, symmetric=True, reorder=order) as dg:
+        got, info = dg.pagerank_pull(0.85, 1e-6, 1000, stats=True)
+        assert np.max(np.abs(got.astype(np.float64) - want)) <= 1e-5
+        out = _dev(g.n, torch.float32)
+        dg.pagerank_pull(0.85, 1e-6, 1000, out=out)
+        assert np.max(np.abs(out.cpu().numpy().astype(np.float64) - want)) <= 1e-5
+        # residual variants against their own oracles; leftover residuals below
+        # tol 1e-4 flow onward with gain alpha/(1-alpha): 2e-3 absolute
+        r, _ = oracle.pr_pull_residual(g, 0.85, 1e-4, 1000)
+        assert np.max(np.abs(dg.pagerank_pull_residual(0.85, 1e-4, 1000).astype(np.float64) - r)) < 2e-3
+        p, _ = oracle.pr_push_sync(g, 0.85, 1e-4, 1000)
+        assert np.max(np.abs(dg.pagerank_push(0.85, 1e-4, 1000).astype(np.float64) - p)) < 2e-3
+
+
+def test_pagerank_reordered_not_converged_still_maps(cuda_device):
+    g, _ = rmat(12, 8, seed=35)
+    with DeviceGraph(g, symmetric=True, reorder=GB_ORDER_DEGREE) as dg:
+        got, info = dg.pagerank_pull(0.85, 0.0, 3, stats=True)
+        assert not info["converged"] and info["iterations"] == 3
+        with DeviceGraph(g, symmetric=True) as plain:
+            ref = plain.pagerank_pull(0.85, 0.0, 3)
+        assert np.max(np.abs(got - ref)) <= 1e-6
+
+
+@pytest.mark.parametrize("batch", [1, 64])
+def test_bc_reordered(cuda_device, batch):
+    g, _ = rmat(11, 8, seed=36)
+    srcs = [int(s) for s in np.random.default_rng(3).choice(g.n, 70, replace=False)]
+    want = oracle.bc_level(g, srcs, f64=True)
+    with DeviceGraph(g, symmetric=True, reorder=GB_ORDER_DEGREE) as dg:
+        got = dg.bc(srcs, batch=batch).astype(np.float64)
+    assert np.max(np.abs(got - want) / np.maximum(1.0, np.abs(want))) <= 1e-5
+
+
+def test_reorder_edge_cases(cuda_device):
+    # single vertex, no arcs
+    g1 = HostCSR.from_edges(1, [], [])
+    with DeviceGraph(g1, symmetric=True, reorder=GB_ORDER_DEGREE) as dg:
+        assert dg.bfs(0).tolist() == [0]
+        assert dg.cc().tolist() == [0]
+    # path whose ids run against degree order
+    n = 50
+    s = list(range(n - 1)) + list(range(1, n))
+    d = list(range(1, n)) + list(range(n - 1))
+    gp = HostCSR.from_edges(n, s, d)
+    with DeviceGraph(gp, symmetric=True, reorder=GB_ORDER_DEGREE) as dg:
+        assert (dg.bfs(0) == np.arange(n)).all()
+        assert (dg.cc() == 0).all()
+
+
+def test_reorder_api_contract(cuda_device):
+    g, _ = rmat(10, 8, seed=37)
+    assign_weights_f32(g, seed=1)
+    packed, first = pack_graphs([g, g])
+    with DeviceGraph(g, symmetric=True) as dg:
+        assert dg.permutation() == {"new_to_old": None, "old_to_new": None}
+        dg.reorder(GB_ORDER_NONE)  # no-op on file order
+        dg.reorder(GB_ORDER_DEGREE)
+        p = dg.permutation()
+        assert p["new_to_old"] and p["old_to_new"]
+        dg.reorder(GB_ORDER_DEGREE)  # same order again: no-op
+        for bad in (GB_ORDER_NONE, GB_ORDER_DEGREE_UNSORTED):
+            with pytest.raises(GbError) as e:
+                dg.reorder(bad)
+            assert e.value.status == _lib.GB_ERR_UNSUPPORTED
+        with pytest.raises(GbError) as e:
+            dg.reorder(7)
+        # PPR needs file order
+        from galois_b200.ppr import ppr
+
+        T = torch.zeros((g.n, 4), dtype=torch.float32, device="cuda")
+        T[0] = 1.0
+        with pytest.raises(GbError) as e:
+            ppr(dg, T, torch.from_numpy(g.w_f32).cuda())
+        assert e.value.status == _lib.GB_ERR_UNSUPPORTED
+    with DeviceGraph(packed, symmetric=True, reorder=GB_ORDER_DEGREE) as dg:
+        with pytest.raises(GbError) as e:
+            dg.multi_graph_bfs_cc(first, np.zeros(2, np.uint32))
+        assert e.value.status == _lib.GB_ERR_UNSUPPORTED
+
+
+def test_autotune_on_reordered(cuda_device, tmp_path):
+    g, perm = rmat(12, 16, seed=38)
+    src = int(perm[0])
+    with DeviceGraph(g, symmetric=True, reorder=GB_ORDER_DEGREE) as dg:
+        dg.autotune("bfs", src, str(tmp_path / "tune.jsonl"))
+        assert (dg.bfs(src) == oracle.bfs_serial(g, src)).all()
