@@ -136,12 +136,13 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(BfsArgs a) {
     for (uint64_t w = gtid; w < words; w += gthreads) fb_cl[w] = 0;
     const uint32_t next_level = L + 1;
 
-    // discovery: all lanes call with their candidate
-    auto discover = [&](bool cand, uint32_t u) {
+    // discovery: all lanes call with their candidate and its visited word
+    // as loaded earlier (a stale word only costs an extra atomicOr)
+    auto discover = [&](bool cand, uint32_t u, uint32_t vw) {
       bool disc = false;
       if (cand) {
         const uint32_t bit = 1u << (u & 31);
-        if (!(a.visited[u >> 5] & bit)) {
+        if (!(vw & bit)) {
           const uint32_t old = atomicOr(&a.visited[u >> 5], bit);
           disc = !(old & bit);
         }
@@ -170,10 +171,10 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(BfsArgs a) {
               d = (uint32_t)(ldg(a.offs + v + 1) - b);
             }
             my_scanned += d;
-            warp_expand(b, d, 0u, [&](bool valid, uint64_t e, uint32_t, uint32_t) {
-              const uint32_t u = valid ? ldg(a.col + e) : 0u;
-              discover(valid, u);
-            });
+            warp_expand_mlp<4, uint32_t>(
+                b, d, 0u, [&](bool valid, uint64_t e, uint32_t) { return valid ? ldg(a.col + e) : 0u; },
+                [&](bool valid, uint64_t, uint32_t u, uint32_t) { return valid ? a.visited[u >> 5] : ~0u; },
+                [&](bool valid, uint32_t, uint32_t, uint32_t u, uint32_t vw) { discover(valid, u, vw); });
           },
           [&](uint32_t t) {
             const uint2 tv = tin[t];
@@ -181,11 +182,20 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(BfsArgs a) {
             const uint64_t b = vb + (uint64_t)tv.y * a.tile;
             const uint64_t e_end = min(ve, b + a.tile);
             if (lane == 0) my_scanned += e_end - b;
-            for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
-              const uint64_t e = e0 + lane;
-              const bool valid = e < e_end;
-              const uint32_t u = valid ? ldg(a.col + e) : 0u;
-              discover(valid, u);
+            constexpr int U = 4;
+            for (uint64_t e0 = b; e0 < e_end; e0 += 32 * U) {
+              uint32_t u[U], vw[U];
+              bool valid[U];
+#pragma unroll
+              for (int k = 0; k < U; ++k) {
+                const uint64_t e = e0 + 32 * k + lane;
+                valid[k] = e < e_end;
+                u[k] = valid[k] ? ldg(a.col + e) : 0u;
+              }
+#pragma unroll
+              for (int k = 0; k < U; ++k) vw[k] = valid[k] ? a.visited[u[k] >> 5] : ~0u;
+#pragma unroll
+              for (int k = 0; k < U; ++k) discover(valid[k], u[k], vw[k]);
             }
           });
     } else {

@@ -59,6 +59,7 @@ struct gb_graph {
   // id (device), h_iperm the host copy for mapping sources; ro_buf holds 3n
   // words of result staging for mapping outputs back to original ids
   int order = 0;
+  uint32_t zero_from = 0;  // degree-ordered: first vertex with no stored arcs (n if none)
   uint32_t* perm = nullptr;
   uint32_t* iperm = nullptr;
   uint32_t* h_iperm = nullptr;

@@ -292,6 +292,7 @@ int gb_graph_upload(const uint64_t* end_offs, const uint32_t* col, const uint32_
             (*flag & 2) ? "last offset != m " : "", (*flag & 4) ? "destination id >= n" : "");
   }
   g->max_degree = *maxdeg;
+  g->zero_from = n;
   *out = g;
   return GB_OK;
 }

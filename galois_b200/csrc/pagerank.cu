@@ -24,6 +24,8 @@
 // arc costs one 4-byte column read and one 4-byte gather, and the L1 change
 // reduced in fp64.  Residual push reuses the frontier queues (frontier.cuh).
 
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "device_graph.cuh"
 #include "frontier.cuh"
@@ -73,6 +75,7 @@ struct PrArgs {
   uint32_t* stamp;
   FrontierQueues fq;
   uint32_t heavy, tile;
+  uint32_t zero_from;  // first vertex of the no-in-arc suffix (degree-ordered graphs), else n
 };
 
 __global__ void count_nout(const uint32_t* __restrict__ col, uint64_t m, uint32_t* nout) {
@@ -108,12 +111,33 @@ __device__ __forceinline__ bool seg_reduce(bool valid, uint32_t owner, float& x)
   return valid && (lane == 0 || kprev != key);
 }
 
-__global__ void __launch_bounds__(kBlock) pr_pull_persistent(PrArgs a) {
-  __shared__ float s_acc[kWarps][32];
+// Sum of gather(col[b .. b+d)) for one row per lane (d <= K): all K column
+// loads, then all K gathers, in flight; arcs are summed in order.
+template <int K, class Gather>
+__device__ __forceinline__ float row_sum(const uint32_t* __restrict__ col, Gather&& gather, uint64_t b, uint32_t d) {
+  uint32_t u[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) u[k] = (uint32_t)k < d ? ldg(col + b + k) : 0u;
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < K; ++k) s += (uint32_t)k < d ? gather(u[k]) : 0.f;
+  return s;
+}
+
+// Jacobi pull iterations, one cooperative persistent launch.  Shared memory
+// is kept small (one float per lane) so that the SM's unified L1/shared array
+// serves as L1 for the gathers; on a degree-ordered graph the hot
+// contributions sit on few lines and stay there.  On such a graph the
+// vertices from zero_from on have no in-arcs, so after two iterations their
+// rank and contribution are constants and their chunks are skipped.
+template <int BLOCK, int U, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) pr_pull_persistent(PrArgs a) {
+  constexpr int kW = BLOCK / 32;
+  __shared__ float s_acc[kW][32];
   PrCtl* ctl = a.ctl;
   const uint64_t deadline = kernel_deadline();
-  const uint64_t gtid = blockIdx.x * (uint64_t)kBlock + threadIdx.x;
-  const uint64_t gthreads = (uint64_t)gridDim.x * kBlock;
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
   const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
   s_acc[wib][lane] = 0.f;
@@ -125,6 +149,7 @@ __global__ void __launch_bounds__(kBlock) pr_pull_persistent(PrArgs a) {
       ctl->l1[(it + 1) % 3] = 0.0;
       ctl->linf[(it + 1) % 3] = 0u;
     }
+    auto gather = [&](uint32_t u) -> float { return c_in[u]; };
     double my_l1 = 0.0;
     float my_max = 0.f;
     auto finish = [&](uint32_t v, float sum) {
@@ -136,33 +161,77 @@ __global__ void __launch_bounds__(kBlock) pr_pull_persistent(PrArgs a) {
       my_l1 += (double)fabsf(value - old);
       my_max = fmaxf(my_max, fabsf(value - old));
     };
-    // 4 steps of (column id, contribution) loads in flight per lane
-    sweep_all_mlp<4, float>(
-        a.offs, a.n, a.sched, gwarp, nwarps,
-        [&](bool valid, uint64_t e, uint32_t) { return valid ? ldg(a.col + e) : 0u; },
-        [&](bool valid, uint64_t, uint32_t u, uint32_t) { return valid ? c_in[u] : 0.f; },
-        [&](bool valid, uint32_t owner, uint32_t, uint32_t, float x) {
-          if (seg_reduce(valid, owner, x)) s_acc[wib][owner] += x;
-          __syncwarp();
-        },
-        [&](uint32_t v, bool valid, bool heavy) {
+    // Tasks: 32-vertex chunks, then heavy-vertex tiles (sweep.cuh's
+    // decomposition).  A chunk whose rows all have at most 16 arcs -- most
+    // chunks of a degree-ordered graph, whose degrees fall monotonically --
+    // runs one row per lane with every column load, then every gather, in
+    // flight and no cross-lane work; other chunks use the warp expansion.
+    const uint64_t nchunks = ((uint64_t)(it >= 2 ? a.zero_from : a.n) + 31) >> 5;  // constant tail skipped
+    const uint64_t total = nchunks + a.sched.ntiles;
+    for (uint64_t t = gwarp; t < total; t += nwarps) {
+      if (t < nchunks) {
+        const uint64_t v = (t << 5) + lane;
+        uint64_t b = 0;
+        uint32_t d = 0;
+        bool heavy = false;
+        if (v < a.n) {
+          b = ldg(a.offs + v);
+          const uint64_t dd = ldg(a.offs + v + 1) - b;
+          heavy = dd > a.sched.heavy;
+          d = heavy ? 0u : (uint32_t)dd;
+        }
+        const uint32_t dmax = __reduce_max_sync(kFull, d);
+        if (dmax <= 4) {
+          const float sum = row_sum<4>(a.col, gather, b, d);
+          if (v < a.n && !heavy) finish((uint32_t)v, sum);
+        } else if (dmax <= 16) {
+          const float sum = row_sum<16>(a.col, gather, b, d);
+          if (v < a.n && !heavy) finish((uint32_t)v, sum);
+        } else {
+          // U steps of (column id, contribution) loads in flight per lane
+          warp_expand_mlp<U, float>(
+              b, d, (uint32_t)v, [&](bool valid, uint64_t e, uint32_t) { return valid ? ldg(a.col + e) : 0u; },
+              [&](bool valid, uint64_t, uint32_t u, uint32_t) { return valid ? gather(u) : 0.f; },
+              [&](bool valid, uint32_t owner, uint32_t, uint32_t, float x) {
+                if (seg_reduce(valid, owner, x)) s_acc[wib][owner] += x;
+                __syncwarp();
+              });
           const float sum = s_acc[wib][lane];
           s_acc[wib][lane] = 0.f;
           __syncwarp();
-          if (valid && !heavy) finish(v, sum);
-        },
-        [&](uint32_t v, uint64_t b, uint64_t e) {
-          float s = 0.f;
-          for (uint64_t i = b + lane; i < e; i += 128) {
-            uint32_t u[4];
+          if (v < a.n && !heavy) finish((uint32_t)v, sum);
+        }
+      } else {
+        // one tile of a heavy row: 8 column loads per lane per round, the
+        // next round's loads issued before this round's gathers are summed
+        const uint2 tv = a.sched.tiles[t - nchunks];
+        const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
+        const uint64_t b = vb + (uint64_t)tv.y * a.sched.tile;
+        const uint64_t e = min(ve, b + a.sched.tile);
+        constexpr int UT = 8;
+        uint32_t u[UT];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) u[k] = i + 32 * k < e ? ldg(a.col + i + 32 * k) : 0xFFFFFFFFu;
+        for (int k = 0; k < UT; ++k) {
+          const uint64_t i = b + lane + 32 * k;
+          u[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
+        }
+        float sum = 0.f;
+        for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
+          uint32_t un[UT];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) s += u[k] != 0xFFFFFFFFu ? c_in[u[k]] : 0.f;
+          for (int k = 0; k < UT; ++k) {
+            const uint64_t i = i0 + 32 * UT + lane + 32 * k;
+            un[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
           }
-          s = warp_sum(s);
-          if (lane == 0) atomicAdd(&a.acc[v], s);
-        });
+#pragma unroll
+          for (int k = 0; k < UT; ++k) sum += u[k] != 0xFFFFFFFFu ? gather(u[k]) : 0.f;
+#pragma unroll
+          for (int k = 0; k < UT; ++k) u[k] = un[k];
+        }
+        sum = warp_sum(sum);
+        if (lane == 0) atomicAdd(&a.acc[tv.x], sum);
+      }
+    }
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     for (uint64_t i = gtid; i < a.sched.nheavy; i += gthreads) {
       const uint32_t v = a.sched.heavy_list[i];
@@ -449,7 +518,8 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
   const void* kfn = nullptr;
   if (kind == PrKind::Pull) {
     pr_pull_init<<<g->sm_count * 4, 256, 0, s>>>(a);
-    kfn = reinterpret_cast<const void*>(&pr_pull_persistent);
+    a.zero_from = g->perm ? g->zero_from : n;
+    kfn = reinterpret_cast<const void*>(&pr_pull_persistent<kBlock, 2, 6>);
   } else if (kind == PrKind::PullResidual) {
     pr_resid_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     GB_CUDA(cudaMemsetAsync(a.acc, 0, sizeof(float) * n, s));

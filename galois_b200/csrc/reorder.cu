@@ -38,6 +38,13 @@ __global__ void degree_ids_kernel(const uint64_t* __restrict__ offs, uint32_t n,
   }
 }
 
+// First index of the (descending) sorted degrees that is zero.
+__global__ void first_zero_kernel(const uint32_t* __restrict__ deg_sorted, uint32_t n, uint32_t* out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+    if (deg_sorted[i] == 0 && (i == 0 || deg_sorted[i - 1] != 0)) atomicMin(out, (uint32_t)i);
+}
+
 __global__ void invert_kernel(const uint32_t* __restrict__ perm, uint32_t n, uint32_t* __restrict__ iperm) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) iperm[perm[i]] = (uint32_t)i;
@@ -269,6 +276,11 @@ int reorder_graph(gb_graph* g, int order, cudaStream_t s) {
   GB_TRY(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 16)));
   GB_TRY(cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, deg, deg2, ids, perm, (int64_t)n, 0, end_bit, s));
   invert_kernel<<<blocks_for(g, n), 256, 0, s>>>(perm, n, iperm);
+  uint32_t* zf = reinterpret_cast<uint32_t*>(ids);  // ids is free after the sort
+  GB_TRY(cudaMemcpyAsync(zf, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  first_zero_kernel<<<blocks_for(g, n), 256, 0, s>>>(deg2, n, zf);
+  uint32_t zero_from = n;
+  GB_TRY(cudaMemcpyAsync(&zero_from, zf, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
 
   // 2. new offsets
   {
@@ -329,6 +341,7 @@ int reorder_graph(gb_graph* g, int order, cudaStream_t s) {
   g->iperm = iperm;
   g->h_iperm = h_iperm;
   g->order = order;
+  g->zero_from = zero_from;
   cleanup(true);
   return reserve_result_bufs(g);
 }

@@ -13,7 +13,13 @@
 //   * per-warp local queues in shared memory: a warp keeps relaxing light
 //     vertices it improved itself for up to `local_depth` rounds inside the
 //     same phase (label-correcting inside the bucket), so high-diameter
-//     graphs need far fewer grid-wide phases; leftovers go to the near queue;
+//     graphs need far fewer grid-wide phases; leftovers go to the near queue.
+//     Local entries are (vertex, distance, begin offset, degree), their
+//     relaxations skipped when popped stale (as the reference's operator
+//     drops a request whose distance is no longer current,
+//     SSSP.cpp:136-142), so they need no stamp and no fence, and a local hop
+//     costs two dependent memory round trips (arcs, then the atomic with the
+//     target's offsets);
 //   * a far pile holding vertices relaxed beyond the bucket (membership
 //     bitmap, so each vertex is in the pile at most once).
 // Work is spread over warps statically (no work-grabbing atomics).  When the
@@ -87,7 +93,7 @@ __global__ void sssp_init(SsspArgs a) {
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
-  __shared__ uint32_t s_lq[BLOCK / 32][kLocalQ];
+  __shared__ uint4 s_lq[BLOCK / 32][kLocalQ];
   SsspCtl* ctl = a.ctl;
   const unsigned nblocks = gridDim.x;
   const uint64_t deadline = kernel_deadline();
@@ -96,7 +102,7 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
   const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
   const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
   const unsigned lanemask_lt = (1u << lane) - 1u;
-  uint32_t* lq = s_lq[threadIdx.x >> 5];
+  uint4* lq = s_lq[threadIdx.x >> 5];
   unsigned long long my_scanned = 0, my_relax = 0;
 
   uint32_t bucket = 0;  // current bucket index; near items have dist < hi
@@ -125,67 +131,79 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
     if (q_light != 0 || q_tiles != 0) {
       // ---- relaxation phase --------------------------------------------
       uint32_t lq_n = 0;  // warp-uniform local queue length
-      // Route improved vertices: light ones into this warp's local queue
-      // while it has room (and local rounds are enabled), the rest into the
-      // near queue; beyond-bucket ones into the far pile.  All lanes call.
-      auto route = [&](bool to_near, bool to_far, uint32_t u) {
-        uint64_t d = 0;
-        // when every vertex is light the exact degree is not needed to bin
-        // it: 1 stands for "light, non-empty" (an empty vertex expands to
-        // nothing, so queueing it costs one idle lane)
-        if (to_near) d = a.all_light ? 1 : ldg(a.offs + u + 1) - ldg(a.offs + u);
-        bool loc = a.local_depth > 0 && to_near && d > 0 && d <= a.heavy;
+      // Route a vertex u this lane just lowered to nd (near: inside the
+      // bucket, far: beyond it; ub/deg: u's begin offset and out-degree, or
+      // 0/1 when they were not needed).  A light near u goes to this warp's
+      // local queue as (u, nd, begin, degree) while there is room, so the
+      // local pop needs no offset loads.  Local entries carry no stamp: when
+      // one is popped and dist[u] has moved below nd its relaxations are
+      // skipped, because whoever moved it routed u again.  Other near
+      // vertices enter the next phase's queue once (the stamp; that entry
+      // reads dist when popped, so it also covers later improvements), far
+      // ones the far pile once (the bitmap).  All lanes call.
+      auto route = [&](bool near, bool far, uint32_t u, uint32_t nd, uint64_t ub, uint64_t deg) {
+        bool loc = a.local_depth > 0 && near && deg > 0 && deg <= a.heavy && deg < 65536 && ub < (1ull << 48);
         const unsigned lm = __ballot_sync(kFull, loc);
         const uint32_t k = __popc(lm);
         if (k) {
           if (lq_n + k <= (uint32_t)kLocalQ) {
-            if (loc) lq[lq_n + __popc(lm & lanemask_lt)] = u;
+            if (loc)
+              lq[lq_n + __popc(lm & lanemask_lt)] =
+                  make_uint4(u, nd, (uint32_t)ub, (uint32_t)((ub >> 32) << 16) | (uint32_t)deg);
             lq_n += k;
             __syncwarp();
           } else {
             loc = false;
           }
         }
-        push_with_degree<false>(a.fq, qnext, nxt, to_near && !loc, u, d, a.heavy, a.tile, &ctl->err);
-        warp_push(to_far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
+        bool to_near = false;
+        if (near && !loc && a.stamp[u] != next_stamp) to_near = atomicExch(&a.stamp[u], next_stamp) != next_stamp;
+        push_with_degree<false>(a.fq, qnext, nxt, to_near, u, deg, a.heavy, a.tile, &ctl->err);
+        warp_push(far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
       };
-      auto relax = [&](bool valid, uint32_t u, uint32_t nd) {
-        bool to_near = false, to_far = false;
-        if (valid && nd < a.dist[u]) {
+      const bool need_deg = !a.all_light || a.local_depth > 0;
+      // du: dist[u] as loaded with the arc, or ~0 to skip the pre-check (a
+      // stale value only costs an extra atomic; the atomicMin decides)
+      auto relax = [&](bool valid, uint32_t u, uint32_t nd, uint32_t du) {
+        bool near = false, far = false;
+        uint64_t ub = 0, deg = 1;
+        if (valid && nd < du) {
+          // the offset loads do not depend on the atomic: issued together
+          if (need_deg) {
+            ub = ldg(a.offs + u);
+            deg = ldg(a.offs + u + 1) - ub;
+          }
           const uint32_t old = atomicMin(&a.dist[u], nd);
           if (nd < old) {
             ++my_relax;
             if (nd < hi) {
-              // fence: the dist update is visible before the stamp is read
-              // (pairs with the fence after a local pop resets the stamp)
-              if (a.local_depth > 0) __threadfence();
-              if (a.stamp[u] != next_stamp) to_near = atomicExch(&a.stamp[u], next_stamp) != next_stamp;
+              near = true;
             } else {
               const uint32_t bit = 1u << (u & 31);
-              if (!(a.infar[u >> 5] & bit)) to_far = !(atomicOr(&a.infar[u >> 5], bit) & bit);
+              if (!(a.infar[u >> 5] & bit)) far = !(atomicOr(&a.infar[u >> 5], bit) & bit);
             }
           }
         }
-        route(to_near, to_far, u);
+        route(near, far, u, nd, ub, deg);
       };
-      // expand one light vertex per lane (has == false: idle lane)
-      auto expand = [&](bool has, uint32_t v) {
-        uint64_t b = 0;
-        uint32_t d = 0, dv = 0;
-        if (has) {
-          b = ldg(a.offs + v);
-          d = (uint32_t)(ldg(a.offs + v + 1) - b);
-          dv = a.dist[v];
-        }
+      // Expand one light vertex per lane: arcs [b, b+d) from distance dv
+      // (d == 0: idle lane).  cur: the vertex's current distance, compared
+      // only when an arc is relaxed, so its load stays off the critical
+      // path; precheck: compare each target's distance before the atomic.
+      auto expand = [&](uint64_t b, uint32_t d, uint32_t dv, uint32_t cur, bool precheck) {
         my_scanned += d;
-        warp_expand(b, d, dv, [&](bool valid, uint64_t e, uint32_t, uint32_t dsrc) {
-          uint32_t u = 0, nd = 0;
-          if (valid) {
-            u = ldg(a.col + e);
-            nd = dsrc + ldg(a.w + e);
-          }
-          relax(valid, u, nd);
-        });
+        // four 32-arc steps in flight per lane: ids, then weights (and the
+        // targets' distances), then the relaxations
+        warp_expand_mlp<4, uint2>(
+            b, d, dv, [&](bool valid, uint64_t e, uint32_t) { return valid ? ldg(a.col + e) : 0u; },
+            [&](bool valid, uint64_t e, uint32_t u, uint32_t dsrc) {
+              return valid ? make_uint2(dsrc + ldg(a.w + e), precheck ? __ldcg(a.dist + u) : 0xFFFFFFFFu)
+                           : make_uint2(0u, 0u);
+            },
+            [&](bool valid, uint32_t owner, uint32_t dsrc, uint32_t u, uint2 v2) {
+              const bool live = __shfl_sync(kFull, cur, owner) >= dsrc;
+              relax(valid && live, u, v2.x, v2.y);
+            });
       };
       const uint32_t* qin = a.fq.light[P & 1];
       const uint2* tin = a.fq.tiles[P & 1];
@@ -194,47 +212,67 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
           [&](uint32_t base, uint32_t vpt) {
             const uint32_t idx = base + lane;
             const bool has = lane < vpt && idx < q_light;
-            expand(has, has ? qin[idx] : 0u);
+            uint64_t b = 0;
+            uint32_t d = 0, dv = 0;
+            if (has) {
+              const uint32_t v = qin[idx];
+              b = ldg(a.offs + v);
+              d = (uint32_t)(ldg(a.offs + v + 1) - b);
+              dv = __ldcg(a.dist + v);
+            }
+            expand(b, d, dv, dv, true);
           },
           [&](uint32_t t) {
             const uint2 tv = tin[t];
             const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
             const uint64_t b = vb + (uint64_t)tv.y * a.tile;
             const uint64_t e_end = min(ve, b + a.tile);
-            const uint32_t dsrc = a.dist[tv.x];
+            const uint32_t dsrc = __ldcg(a.dist + tv.x);
             if (lane == 0) my_scanned += e_end - b;
-            for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
-              const uint64_t e = e0 + lane;
-              const bool valid = e < e_end;
-              uint32_t u = 0, nd = 0;
-              if (valid) {
-                u = ldg(a.col + e);
-                nd = dsrc + ldg(a.w + e);
+            constexpr int U = 4;
+            for (uint64_t e0 = b; e0 < e_end; e0 += 32 * U) {
+              uint32_t u[U], nd[U], du[U];
+              bool valid[U];
+#pragma unroll
+              for (int k = 0; k < U; ++k) {
+                const uint64_t e = e0 + 32 * k + lane;
+                valid[k] = e < e_end;
+                u[k] = valid[k] ? ldg(a.col + e) : 0u;
               }
-              relax(valid, u, nd);
+#pragma unroll
+              for (int k = 0; k < U; ++k) {
+                const uint64_t e = e0 + 32 * k + lane;
+                nd[k] = valid[k] ? dsrc + ldg(a.w + e) : 0u;
+                du[k] = valid[k] ? __ldcg(a.dist + u[k]) : 0u;
+              }
+#pragma unroll
+              for (int k = 0; k < U; ++k) relax(valid[k], u[k], nd[k], du[k]);
             }
           });
-      // local rounds: keep relaxing what this warp improved (LIFO)
+      // local rounds: keep relaxing what this warp lowered (LIFO), with no
+      // distance pre-check (low-degree targets: the atomic is cheaper than
+      // another dependent load)
       for (int r = 0; r < a.local_depth && lq_n > 0; ++r) {
         const uint32_t take = min(32u, lq_n);
         const bool has = lane < take;
-        const uint32_t v = has ? lq[lq_n - take + lane] : 0u;
+        const uint4 ent = has ? lq[lq_n - take + lane] : make_uint4(0u, 0u, 0u, 0u);
         __syncwarp();
         lq_n -= take;
-        if (has) {
-          a.stamp[v] = kNotQueued;  // from here an improvement re-queues v
-          __threadfence();
-        }
-        expand(has, v);
+        const uint64_t b = ((uint64_t)(ent.w >> 16) << 32) | ent.z;
+        const uint32_t cur = has ? __ldcg(a.dist + ent.x) : 0u;
+        expand(b, ent.w & 0xFFFFu, ent.y, cur, false);
       }
-      // leftovers go to the near queue; they keep their stamp P+1
+      // leftovers that are still current join the next phase's near queue
       while (lq_n > 0) {
         const uint32_t take = min(32u, lq_n);
         const bool has = lane < take;
-        const uint32_t v = has ? lq[lq_n - take + lane] : 0u;
+        const uint4 ent = has ? lq[lq_n - take + lane] : make_uint4(0u, 0u, 0u, 0u);
         __syncwarp();
         lq_n -= take;
-        push_discovered<false>(a.fq, qnext, nxt, has, v, a.offs, a.heavy, a.tile, &ctl->err);
+        bool to_near = false;
+        if (has && __ldcg(a.dist + ent.x) >= ent.y && a.stamp[ent.x] != next_stamp)
+          to_near = atomicExch(&a.stamp[ent.x], next_stamp) != next_stamp;
+        push_discovered<false>(a.fq, qnext, nxt, to_near, ent.x, a.offs, a.heavy, a.tile, &ctl->err);
       }
       if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
       ++P;
