@@ -15,10 +15,14 @@
 //        discovery = check-before-atomicOr on a visited bitmap (2 MB for 16M
 //        vertices, L2 resident), warp-aggregated queue appends;
 //   pull (bottom-up): every unvisited vertex scans its in-edges until it finds
-//        a parent in the frontier bitmap.
-// Every discovered vertex is written to both the next queue and the next
-// frontier bitmap, so either direction can follow without a conversion pass.
-// Levels are separated by a bounded software grid barrier.
+//        a parent in the frontier bitmap; a warp owns one bitmap word, so the
+//        visited and next-frontier words are written with plain stores.
+// Every level writes the next frontier bitmap; push levels also fill the
+// next queue, and a push level that follows a pull level first converts the
+// bitmap into the queue.  The frontier totals that drive the direction switch
+// are summed per CTA and added to the global counters once per CTA, so no
+// counter is hit by every warp.  Levels are separated by a bounded software
+// grid barrier.
 
 #include "device_common.cuh"
 #include "device_graph.cuh"
@@ -100,21 +104,26 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(BfsArgs a) {
   uint32_t old_items = 0;
   unsigned long long my_scanned = 0;
 
+  // per-level totals of the next frontier, summed per CTA in shared memory
+  // and added to the global counters once per CTA
+  __shared__ unsigned long long s_cnt[2];
+  __shared__ uint32_t s_stage[BLOCK / 32][64];
+  if (threadIdx.x == 0) s_cnt[0] = s_cnt[1] = 0;
+  __syncthreads();
+
   for (uint32_t L = 0;; ++L) {
     const int rd = L % 3, wr = (L + 1) % 3, cl = (L + 2) % 3;
     FrontierCounters& cur = ctl->fc[rd];
     FrontierCounters& nxt = ctl->fc[wr];
-    // counts can exceed capacity only after an overflow (error raised); clamp reads
-    const uint32_t q_light = min(cur.light, a.fq.light_cap);
-    const uint32_t q_tiles = min(cur.tiles, a.fq.tile_cap);
     const uint32_t items = cur.vertices;
     const unsigned long long scout = cur.degree_sum;
-    if (q_light == 0 && q_tiles == 0) break;
+    if (scout == 0) break;  // no frontier vertex has an arc: nothing left to find
     if (L >= a.max_levels) {
       if (gtid == 0) raise_err(&ctl->err, kDevMaxRounds);
       break;
     }
     // choose the direction for this level
+    const int prev_pull = pull;
     if (can_pull) {
       if (!pull) {
         if ((double)scout > (double)edges_to_check / a.alpha) { pull = 1; old_items = 0; }
@@ -135,26 +144,53 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(BfsArgs a) {
     uint32_t* fb_cl = a.fbits[cl];
     for (uint64_t w = gtid; w < words; w += gthreads) fb_cl[w] = 0;
     const uint32_t next_level = L + 1;
-
-    // discovery: all lanes call with their candidate and its visited word
-    // as loaded earlier (a stale word only costs an extra atomicOr)
-    auto discover = [&](bool cand, uint32_t u, uint32_t vw) {
-      bool disc = false;
-      if (cand) {
-        const uint32_t bit = 1u << (u & 31);
-        if (!(vw & bit)) {
-          const uint32_t old = atomicOr(&a.visited[u >> 5], bit);
-          disc = !(old & bit);
-        }
-        if (disc) {
-          a.level[u] = next_level;
-          atomicOr(&fb_wr[u >> 5], bit);
-        }
-      }
-      push_discovered(a.fq, (L + 1) & 1, nxt, disc, u, a.offs, a.heavy, a.tile, &ctl->err);
-    };
+    uint32_t my_items = 0;
+    unsigned long long my_deg = 0;
 
     if (!pull) {
+      // A pull level leaves only the frontier bitmap; a push level after it
+      // first turns the bitmap into the queue.
+      if (prev_pull) {
+        for (uint64_t base = gtid - lane; base < words; base += gthreads) {
+          const uint64_t w = base + lane;
+          uint32_t bits = w < words ? fb_rd[w] : 0u;
+          while (__any_sync(kFull, bits != 0)) {
+            const bool has = bits != 0;
+            const uint32_t v = has ? (uint32_t)(w << 5) + (uint32_t)(__ffs(bits) - 1) : 0u;
+            bits &= bits - 1;
+            push_discovered<false>(a.fq, L & 1, cur, has, v, a.offs, a.heavy, a.tile, &ctl->err);
+          }
+        }
+        if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+      }
+      const uint32_t q_light = min(cur.light, a.fq.light_cap);
+      const uint32_t q_tiles = min(cur.tiles, a.fq.tile_cap);
+      WarpStage<64> stage{s_stage[threadIdx.x >> 5], 0u};  // light appends, published per 64
+      uint32_t* const nq = a.fq.light[(L + 1) & 1];
+      // discovery: all lanes call with their candidate and its visited word
+      // as loaded earlier (a stale word only costs an extra atomicOr)
+      auto discover = [&](bool cand, uint32_t u, uint32_t vw) {
+        bool disc = false;
+        if (cand) {
+          const uint32_t bit = 1u << (u & 31);
+          if (!(vw & bit)) {
+            const uint32_t old = atomicOr(&a.visited[u >> 5], bit);
+            disc = !(old & bit);
+          }
+          if (disc) {
+            a.level[u] = next_level;
+            atomicOr(&fb_wr[u >> 5], bit);
+          }
+        }
+        if (__any_sync(kFull, disc)) {  // most steps discover nothing
+          uint64_t d = 0;
+          if (disc) d = ldg(a.offs + u + 1) - ldg(a.offs + u);
+          my_items += disc ? 1u : 0u;
+          my_deg += d;
+          stage.push(disc && d > 0 && d <= a.heavy, u, nq, &nxt.light, a.fq.light_cap, &ctl->err);
+          push_with_degree<false>(a.fq, (L + 1) & 1, nxt, disc && d > a.heavy, u, d, a.heavy, a.tile, &ctl->err);
+        }
+      };
       const uint32_t* qin = a.fq.light[L & 1];
       const uint2* tin = a.fq.tiles[L & 1];
       // light vertices 32 per task, heavy vertices' edge tiles one per task,
@@ -198,36 +234,54 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(BfsArgs a) {
               for (int k = 0; k < U; ++k) discover(valid[k], u[k], vw[k]);
             }
           });
+      stage.flush(nq, &nxt.light, a.fq.light_cap, &ctl->err);
     } else {
-      // bottom-up over all vertices; warp-uniform trip count
+      // Bottom-up over all vertices; warp-uniform trip count.  A warp owns
+      // the 32 vertices of one bitmap word and is the only writer of that
+      // word of `visited` and of the next frontier in a pull level, so both
+      // are written with plain stores of the warp's ballot.  The next
+      // frontier is left as a bitmap (no queue).
       for (uint64_t base = gtid - lane; base < a.n; base += gthreads) {
         const uint64_t u64 = base + lane;
         bool found = false;
-        uint32_t u = (uint32_t)u64;
-        if (u64 < a.n) {
-          const uint32_t bit = 1u << (u & 31);
-          if (!(a.visited[u >> 5] & bit)) {
-            const uint64_t b = ldg(a.in_offs + u), e = ldg(a.in_offs + u + 1);
-            uint64_t i = b;
-            for (; i < e; ++i) {
-              const uint32_t p = ldg(a.in_col + i);
-              if (fb_rd[p >> 5] & (1u << (p & 31))) { found = true; ++i; break; }
-            }
-            my_scanned += i - b;
+        const uint32_t u = (uint32_t)u64;
+        const uint32_t vword = base < a.n ? a.visited[base >> 5] : ~0u;
+        if (u64 < a.n && !(vword & (1u << lane))) {
+          const uint64_t b = ldg(a.in_offs + u), e = ldg(a.in_offs + u + 1);
+          uint64_t i = b;
+          for (; i < e; ++i) {
+            const uint32_t p = ldg(a.in_col + i);
+            if (fb_rd[p >> 5] & (1u << (p & 31))) { found = true; ++i; break; }
           }
+          my_scanned += i - b;
         }
-        bool disc = false;
-        if (found) {
-          const uint32_t bit = 1u << (u & 31);
-          const uint32_t old = atomicOr(&a.visited[u >> 5], bit);
-          disc = !(old & bit);
-          if (disc) {
+        const uint32_t m = __ballot_sync(kFull, found);
+        if (m) {
+          if (lane == 0) {
+            a.visited[base >> 5] = vword | m;
+            fb_wr[base >> 5] = m;
+          }
+          if (found) {
             a.level[u] = next_level;
-            atomicOr(&fb_wr[u >> 5], bit);
+            my_items += 1;
+            my_deg += ldg(a.offs + u + 1) - ldg(a.offs + u);
           }
         }
-        push_discovered(a.fq, (L + 1) & 1, nxt, disc, u, a.offs, a.heavy, a.tile, &ctl->err);
       }
+    }
+    my_items = warp_sum(my_items);
+    my_deg = warp_sum(my_deg);
+    if (lane == 0 && my_items) {
+      atomicAdd(&s_cnt[0], (unsigned long long)my_items);
+      atomicAdd(&s_cnt[1], my_deg);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (s_cnt[0]) {
+        atomicAdd(&nxt.vertices, (uint32_t)s_cnt[0]);
+        atomicAdd(&nxt.degree_sum, s_cnt[1]);
+      }
+      s_cnt[0] = s_cnt[1] = 0;
     }
     if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
     if (gtid == 0) {

@@ -109,6 +109,42 @@ __device__ __forceinline__ void push_discovered(const FrontierQueues& q, int qb,
   push_with_degree<kCount>(q, qb, c, disc, u, d, heavy, tile, err);
 }
 
+// Per-warp staging of light-queue appends in shared memory.  Appends collect
+// in `slots` (K entries owned by one warp) and are published with one
+// atomicAdd per flush instead of one per warp step, so a queue counter that
+// every warp appends to is touched K/32 times less often.  `n` is
+// warp-uniform; every call is warp-collective.
+template <int K>
+struct WarpStage {
+  uint32_t* slots;
+  uint32_t n;
+
+  __device__ __forceinline__ void flush(uint32_t* queue, uint32_t* count, uint32_t cap, int* err) {
+    if (n == 0) return;
+    const uint32_t lane = lane_id();
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(count, n);
+    base = __shfl_sync(kFull, base, 0);
+    for (uint32_t i = lane; i < n; i += 32) {
+      if (base + i < cap) queue[base + i] = slots[i];
+      else raise_err(err, kDevOverflow);
+    }
+    __syncwarp();
+    n = 0;
+  }
+
+  __device__ __forceinline__ void push(bool pred, uint32_t item, uint32_t* queue, uint32_t* count, uint32_t cap,
+                                       int* err) {
+    const unsigned mask = __ballot_sync(kFull, pred);
+    if (!mask) return;
+    const uint32_t k = __popc(mask);
+    if (n + k > (uint32_t)K) flush(queue, count, cap, err);
+    if (pred) slots[n + __popc(mask & ((1u << lane_id()) - 1u))] = item;
+    n += k;
+    __syncwarp();
+  }
+};
+
 // Vertices per light task: 32 when the frontier fills every warp, fewer
 // (a power of two) for small frontiers so that more warps share them and the
 // per-phase critical path is one expansion step instead of several.

@@ -37,6 +37,7 @@ namespace gb {
 namespace {
 
 constexpr int kLocalQ = 64;  // local-queue entries per warp
+constexpr int kStage = 64;   // near-queue appends staged per warp before publishing
 constexpr uint32_t kNotQueued = 0xFFFFFFFFu;
 
 struct SsspCtl {
@@ -94,6 +95,7 @@ __global__ void sssp_init(SsspArgs a) {
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
   __shared__ uint4 s_lq[BLOCK / 32][kLocalQ];
+  __shared__ uint32_t s_stage[BLOCK / 32][kStage];
   SsspCtl* ctl = a.ctl;
   const unsigned nblocks = gridDim.x;
   const uint64_t deadline = kernel_deadline();
@@ -131,6 +133,8 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
     if (q_light != 0 || q_tiles != 0) {
       // ---- relaxation phase --------------------------------------------
       uint32_t lq_n = 0;  // warp-uniform local queue length
+      WarpStage<kStage> stage{s_stage[threadIdx.x >> 5], 0u};
+      uint32_t* const nq = a.fq.light[qnext];
       // Route a vertex u this lane just lowered to nd (near: inside the
       // bucket, far: beyond it; ub/deg: u's begin offset and out-degree, or
       // 0/1 when they were not needed).  A light near u goes to this warp's
@@ -142,6 +146,7 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
       // reads dist when popped, so it also covers later improvements), far
       // ones the far pile once (the bitmap).  All lanes call.
       auto route = [&](bool near, bool far, uint32_t u, uint32_t nd, uint64_t ub, uint64_t deg) {
+        if (!__any_sync(kFull, near || far)) return;  // most steps lower nothing
         bool loc = a.local_depth > 0 && near && deg > 0 && deg <= a.heavy && deg < 65536 && ub < (1ull << 48);
         const unsigned lm = __ballot_sync(kFull, loc);
         const uint32_t k = __popc(lm);
@@ -158,7 +163,8 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
         }
         bool to_near = false;
         if (near && !loc && a.stamp[u] != next_stamp) to_near = atomicExch(&a.stamp[u], next_stamp) != next_stamp;
-        push_with_degree<false>(a.fq, qnext, nxt, to_near, u, deg, a.heavy, a.tile, &ctl->err);
+        stage.push(to_near && deg > 0 && deg <= a.heavy, u, nq, &nxt.light, a.fq.light_cap, &ctl->err);
+        push_with_degree<false>(a.fq, qnext, nxt, to_near && deg > a.heavy, u, deg, a.heavy, a.tile, &ctl->err);
         warp_push(far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
       };
       const bool need_deg = !a.all_light || a.local_depth > 0;
@@ -272,8 +278,9 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
         bool to_near = false;
         if (has && __ldcg(a.dist + ent.x) >= ent.y && a.stamp[ent.x] != next_stamp)
           to_near = atomicExch(&a.stamp[ent.x], next_stamp) != next_stamp;
-        push_discovered<false>(a.fq, qnext, nxt, to_near, ent.x, a.offs, a.heavy, a.tile, &ctl->err);
+        stage.push(to_near, ent.x, nq, &nxt.light, a.fq.light_cap, &ctl->err);  // local entries are light
       }
+      stage.flush(nq, &nxt.light, a.fq.light_cap, &ctl->err);
       if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
       ++P;
       continue;
