@@ -143,8 +143,31 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
         },
         [&](uint32_t, bool, bool) {},
         [&](uint32_t v, uint64_t b, uint64_t e) {
+          // one tile of a heavy row: 8 column loads, then 8 label loads, per lane
           if (lane == 0) my_scanned += e - b;
-          for (uint64_t i = b + lane; i < e; i += 32) hook(true, v, ldg(a.col + i));
+          const uint32_t pv = a.p[v];
+          constexpr int UT = 8;
+          for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
+            uint32_t u[UT], pu[UT];
+#pragma unroll
+            for (int k = 0; k < UT; ++k) {
+              const uint64_t i = i0 + lane + 32 * k;
+              const uint32_t x = i < e ? ldg(a.col + i) : 0u;
+              u[k] = (i < e && (!a.half || x > v)) ? x : 0xFFFFFFFFu;
+            }
+#pragma unroll
+            for (int k = 0; k < UT; ++k) pu[k] = u[k] != 0xFFFFFFFFu ? a.p[u[k]] : 0u;
+#pragma unroll
+            for (int k = 0; k < UT; ++k) {
+              if (u[k] != 0xFFFFFFFFu && pv != pu[k]) {
+                const uint32_t hi = max(pv, pu[k]), lo = min(pv, pu[k]);
+                if (lo < a.p[hi]) {
+                  atomicMin(&a.p[hi], lo);
+                  my_change = true;
+                }
+              }
+            }
+          }
         });
     if (__any_sync(kFull, my_change) && lane == 0) atomicOr(changed, 1u);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;

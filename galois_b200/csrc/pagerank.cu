@@ -111,19 +111,6 @@ __device__ __forceinline__ bool seg_reduce(bool valid, uint32_t owner, float& x)
   return valid && (lane == 0 || kprev != key);
 }
 
-// Sum of gather(col[b .. b+d)) for one row per lane (d <= K): all K column
-// loads, then all K gathers, in flight; arcs are summed in order.
-template <int K, class Gather>
-__device__ __forceinline__ float row_sum(const uint32_t* __restrict__ col, Gather&& gather, uint64_t b, uint32_t d) {
-  uint32_t u[K];
-#pragma unroll
-  for (int k = 0; k < K; ++k) u[k] = (uint32_t)k < d ? ldg(col + b + k) : 0u;
-  float s = 0.f;
-#pragma unroll
-  for (int k = 0; k < K; ++k) s += (uint32_t)k < d ? gather(u[k]) : 0.f;
-  return s;
-}
-
 // Jacobi pull iterations, one cooperative persistent launch.  Shared memory
 // is kept small (one float per lane) so that the SM's unified L1/shared array
 // serves as L1 for the gathers; on a degree-ordered graph the hot
@@ -161,11 +148,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_persistent(PrArgs a) {
       my_l1 += (double)fabsf(value - old);
       my_max = fmaxf(my_max, fabsf(value - old));
     };
-    // Tasks: 32-vertex chunks, then heavy-vertex tiles (sweep.cuh's
-    // decomposition).  A chunk whose rows all have at most 16 arcs -- most
-    // chunks of a degree-ordered graph, whose degrees fall monotonically --
-    // runs one row per lane with every column load, then every gather, in
-    // flight and no cross-lane work; other chunks use the warp expansion.
+    // Tasks: 32-vertex chunks (warp expansion, U steps of loads in flight;
+    // a chunk without arcs only finishes its vertices), then heavy-vertex
+    // tiles (sweep.cuh's decomposition).
     const uint64_t nchunks = ((uint64_t)(it >= 2 ? a.zero_from : a.n) + 31) >> 5;  // constant tail skipped
     const uint64_t total = nchunks + a.sched.ntiles;
     for (uint64_t t = gwarp; t < total; t += nwarps) {
@@ -181,12 +166,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_persistent(PrArgs a) {
           d = heavy ? 0u : (uint32_t)dd;
         }
         const uint32_t dmax = __reduce_max_sync(kFull, d);
-        if (dmax <= 4) {
-          const float sum = row_sum<4>(a.col, gather, b, d);
-          if (v < a.n && !heavy) finish((uint32_t)v, sum);
-        } else if (dmax <= 16) {
-          const float sum = row_sum<16>(a.col, gather, b, d);
-          if (v < a.n && !heavy) finish((uint32_t)v, sum);
+        if (dmax == 0) {
+          if (v < a.n && !heavy) finish((uint32_t)v, 0.f);
         } else {
           // U steps of (column id, contribution) loads in flight per lane
           warp_expand_mlp<U, float>(
