@@ -110,65 +110,72 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
     uint32_t* changed = &ctl->changed[r % 3];
     if (gtid == 0) ctl->changed[(r + 1) % 3] = 0;
     bool my_change = false;
-    auto hook = [&](bool valid, uint32_t v, uint32_t u) {
-      if (valid && (!a.half || u > v)) {
-        const uint32_t pv = a.p[v], pu = a.p[u];
-        if (pv != pu) {
-          const uint32_t hi = max(pv, pu), lo = min(pv, pu);
-          if (lo < a.p[hi]) {
-            atomicMin(&a.p[hi], lo);
-            my_change = true;
-          }
+    // Hook labels pv (of v, read once per vertex; a stale value is still a
+    // label of v's component, so the union stays valid) and pu: the larger
+    // goes under the smaller, checked before the atomic.
+    auto hook = [&](bool valid, uint32_t pv, uint32_t pu) {
+      if (valid && pv != pu) {
+        const uint32_t hi = max(pv, pu), lo = min(pv, pu);
+        if (lo < a.p[hi]) {
+          atomicMin(&a.p[hi], lo);
+          my_change = true;
         }
       }
     };
-    // 4 steps of (column, label) loads in flight per lane
-    sweep_all_mlp<4, uint32_t>(
-        a.offs, a.n, a.sched, gwarp, nwarps,
-        [&](bool valid, uint64_t e, uint32_t v) {
-          const uint32_t u = valid ? ldg(a.col + e) : 0u;
-          return (valid && (!a.half || u > v)) ? u : 0xFFFFFFFFu;
-        },
-        [&](bool, uint64_t, uint32_t u, uint32_t) { return u != 0xFFFFFFFFu ? a.p[u] : 0u; },
-        [&](bool, uint32_t, uint32_t v, uint32_t u, uint32_t pu) {
-          if (u == 0xFFFFFFFFu) return;
-          const uint32_t pv = a.p[v];
-          if (pv != pu) {
-            const uint32_t hi = max(pv, pu), lo = min(pv, pu);
-            if (lo < a.p[hi]) {
-              atomicMin(&a.p[hi], lo);
-              my_change = true;
-            }
-          }
-        },
-        [&](uint32_t, bool, bool) {},
-        [&](uint32_t v, uint64_t b, uint64_t e) {
-          // one tile of a heavy row: 8 column loads, then 8 label loads, per lane
-          if (lane == 0) my_scanned += e - b;
-          const uint32_t pv = a.p[v];
-          constexpr int UT = 8;
-          for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
-            uint32_t u[UT], pu[UT];
+    // Tasks as in sweep.cuh: 32-vertex chunks, then heavy-vertex tiles.  In
+    // a chunk each lane reads its vertex's label once; the expansion (4 steps
+    // of column and label loads in flight) takes the owner's label by shuffle.
+    const uint64_t nchunks = ((uint64_t)a.n + 31) >> 5;
+    const uint64_t total = nchunks + a.sched.ntiles;
+    // one tile of a heavy row: 8 column loads, then 8 label loads, per lane
+    auto tile_fn = [&](uint32_t v, uint64_t b, uint64_t e) {
+      if (lane == 0) my_scanned += e - b;
+      const uint32_t pv = a.p[v];
+      constexpr int UT = 8;
+      for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
+        uint32_t u[UT], pu[UT];
 #pragma unroll
-            for (int k = 0; k < UT; ++k) {
-              const uint64_t i = i0 + lane + 32 * k;
-              const uint32_t x = i < e ? ldg(a.col + i) : 0u;
-              u[k] = (i < e && (!a.half || x > v)) ? x : 0xFFFFFFFFu;
-            }
+        for (int k = 0; k < UT; ++k) {
+          const uint64_t i = i0 + lane + 32 * k;
+          const uint32_t x = i < e ? ldg(a.col + i) : 0u;
+          u[k] = (i < e && (!a.half || x > v)) ? x : 0xFFFFFFFFu;
+        }
 #pragma unroll
-            for (int k = 0; k < UT; ++k) pu[k] = u[k] != 0xFFFFFFFFu ? a.p[u[k]] : 0u;
+        for (int k = 0; k < UT; ++k) pu[k] = u[k] != 0xFFFFFFFFu ? a.p[u[k]] : 0u;
 #pragma unroll
-            for (int k = 0; k < UT; ++k) {
-              if (u[k] != 0xFFFFFFFFu && pv != pu[k]) {
-                const uint32_t hi = max(pv, pu[k]), lo = min(pv, pu[k]);
-                if (lo < a.p[hi]) {
-                  atomicMin(&a.p[hi], lo);
-                  my_change = true;
-                }
-              }
-            }
-          }
-        });
+        for (int k = 0; k < UT; ++k) hook(u[k] != 0xFFFFFFFFu, pv, pu[k]);
+      }
+    };
+    for (uint64_t t = gwarp; t < total; t += nwarps) {
+      if (t < nchunks) {
+        const uint64_t v64 = (t << 5) + lane;
+        uint64_t b = 0;
+        uint32_t d = 0, pv = 0;
+        if (v64 < a.n) {
+          b = ldg(a.offs + v64);
+          const uint64_t dd = ldg(a.offs + v64 + 1) - b;
+          d = dd > a.sched.heavy ? 0u : (uint32_t)dd;
+          pv = a.p[v64];
+        }
+        my_scanned += d;
+        warp_expand_mlp<4, uint32_t>(
+            b, d, (uint32_t)v64,
+            [&](bool valid, uint64_t e, uint32_t v) {
+              const uint32_t u = valid ? ldg(a.col + e) : 0u;
+              return (valid && (!a.half || u > v)) ? u : 0xFFFFFFFFu;
+            },
+            [&](bool, uint64_t, uint32_t u, uint32_t) { return u != 0xFFFFFFFFu ? a.p[u] : 0u; },
+            [&](bool, uint32_t owner, uint32_t, uint32_t u, uint32_t pu) {
+              const uint32_t opv = __shfl_sync(kFull, pv, owner);
+              hook(u != 0xFFFFFFFFu, opv, pu);
+            });
+      } else {
+        const uint2 tv = a.sched.tiles[t - nchunks];
+        const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
+        const uint64_t tb = vb + (uint64_t)tv.y * a.sched.tile;
+        tile_fn(tv.x, tb, min(ve, tb + a.sched.tile));
+      }
+    }
     if (__any_sync(kFull, my_change) && lane == 0) atomicOr(changed, 1u);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     compress_all(a, gtid, gthreads);
