@@ -281,7 +281,7 @@ class BfsJob(Job):
         super().__init__(size)
         from galois_b200 import rmat
 
-        scale = pick(size, 16, 18, 20, 24)
+        scale = pick(size, 16, 21, 20, 24)
         self.workload = self.workload.replace("RMAT-20", f"RMAT-{scale}")
         g, _ = rmat(scale, 16, seed=20, symmetrize=True)
         self.graphs.append({"name": f"rmat{scale}-sym", "host": g, "symmetric": True,
@@ -657,7 +657,8 @@ def main() -> None:
     stats = st_runs[-1]
     units_step = sum(job.units(st, gi) for gi, st in enumerate(stats))
     bytes_step = sum(job.algo_bytes(st, gi) for gi, st in enumerate(stats))
-    kms = [sum(r[gi]["kernel_ms"] for r in st_runs) / len(st_runs) for gi in range(len(dgs))]
+    # the first call of a kernel also pays its lazy module load: average the later runs
+    kms = [sum(r[gi]["kernel_ms"] for r in st_runs[1:]) / (len(st_runs) - 1) for gi in range(len(dgs))]
     for _ in range(args.warmup):
         for gi, dg in enumerate(dgs):
             job.device_call(dg, gi, outs[gi])
