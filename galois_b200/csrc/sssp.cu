@@ -203,7 +203,8 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
         warp_expand_mlp<4, uint2>(
             b, d, dv, [&](bool valid, uint64_t e, uint32_t) { return valid ? ldg(a.col + e) : 0u; },
             [&](bool valid, uint64_t e, uint32_t u, uint32_t dsrc) {
-              return valid ? make_uint2(dsrc + ldg(a.w + e), precheck ? __ldcg(a.dist + u) : 0xFFFFFFFFu)
+              // the pre-check may read a stale (cached, never smaller) value
+              return valid ? make_uint2(dsrc + ldg(a.w + e), precheck ? a.dist[u] : 0xFFFFFFFFu)
                            : make_uint2(0u, 0u);
             },
             [&](bool valid, uint32_t owner, uint32_t dsrc, uint32_t u, uint2 v2) {
@@ -249,7 +250,7 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
               for (int k = 0; k < U; ++k) {
                 const uint64_t e = e0 + 32 * k + lane;
                 nd[k] = valid[k] ? dsrc + ldg(a.w + e) : 0u;
-                du[k] = valid[k] ? __ldcg(a.dist + u[k]) : 0u;
+                du[k] = valid[k] ? a.dist[u[k]] : 0u;
               }
 #pragma unroll
               for (int k = 0; k < U; ++k) relax(valid[k], u[k], nd[k], du[k]);
