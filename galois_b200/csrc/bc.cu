@@ -410,13 +410,7 @@ __global__ void __launch_bounds__(kBcBlock) ss_persistent(SsArgs a) {
         uint64_t d = 0;
         if (disc) d = ldg(a.offs + u + 1) - ldg(a.offs + u);
         const uint32_t nt = (disc && d > a.heavy) ? (uint32_t)((d + a.tile - 1) / a.tile) : 0u;
-        if (__ballot_sync(kFull, nt != 0)) {
-          const uint32_t first = warp_reserve(nt, &a.tails[1]);
-          for (uint32_t k = 0; k < nt; ++k) {
-            if (first + k < a.tile_cap) a.tiles[first + k] = make_uint2(u, k);
-            else raise_err(&ctl->err, kDevOverflow);
-          }
-        }
+        warp_push_tiles(u, nt, a.tiles, &a.tails[1], a.tile_cap, &ctl->err);
       }
     };
     for_each_frontier_task(

@@ -135,6 +135,28 @@ __device__ __forceinline__ uint32_t warp_reserve(uint32_t k, uint32_t* count) {
   return base + incl - k;
 }
 
+// Warp-collective: every lane with nt > 0 appends tiles (v, 0) .. (v, nt-1)
+// to `tiles`, reserved with one atomic per warp.  The whole warp writes each
+// lane's run in turn (32 coalesced stores per step), so a lane holding a
+// vertex of very high degree does not write its run alone.
+__device__ __forceinline__ void warp_push_tiles(uint32_t v, uint32_t nt, uint2* tiles, uint32_t* count,
+                                                uint32_t cap, int* err) {
+  unsigned m = __ballot_sync(kFull, nt != 0);
+  if (!m) return;
+  const uint32_t first = warp_reserve(nt, count);
+  const uint32_t lane = lane_id();
+  for (; m; m &= m - 1) {
+    const int src = __ffs(m) - 1;
+    const uint32_t f = __shfl_sync(kFull, first, src);
+    const uint32_t cnt = __shfl_sync(kFull, nt, src);
+    const uint32_t vv = __shfl_sync(kFull, v, src);
+    for (uint32_t k = lane; k < cnt; k += 32) {
+      if (f + k < cap) tiles[f + k] = make_uint2(vv, k);
+      else raise_err(err, kDevOverflow);
+    }
+  }
+}
+
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

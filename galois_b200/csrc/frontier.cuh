@@ -79,15 +79,7 @@ __device__ __forceinline__ void push_with_degree(const FrontierQueues& q, int qb
   const bool light = disc && d > 0 && d <= heavy;
   const bool hv = disc && d > heavy;
   warp_push(light, u, q.light[qb], &c.light, q.light_cap, err);
-  const unsigned hmask = __ballot_sync(kFull, hv);
-  if (hmask) {
-    const uint32_t nt = hv ? (uint32_t)((d + tile - 1) / tile) : 0u;
-    const uint32_t first = warp_reserve(nt, &c.tiles);
-    for (uint32_t k = 0; k < nt; ++k) {
-      if (first + k < q.tile_cap) q.tiles[qb][first + k] = make_uint2(u, k);
-      else raise_err(err, kDevOverflow);
-    }
-  }
+  warp_push_tiles(u, hv ? (uint32_t)((d + tile - 1) / tile) : 0u, q.tiles[qb], &c.tiles, q.tile_cap, err);
   if (kCount) {
     const unsigned dmask = __ballot_sync(kFull, disc);
     if (dmask) {

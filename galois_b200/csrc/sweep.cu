@@ -19,14 +19,7 @@ __global__ void sweep_tiles_kernel(const uint64_t* __restrict__ offs, uint32_t n
     if (v < n) d = offs[v + 1] - offs[v];
     const bool hv = v < n && d > heavy;
     warp_push(hv, (uint32_t)v, heavy_list, &counts[1], heavy_cap, err);
-    const uint32_t nt = hv ? (uint32_t)((d + tile - 1) / tile) : 0u;
-    if (__ballot_sync(kFull, nt != 0)) {
-      const uint32_t first = warp_reserve(nt, &counts[0]);
-      for (uint32_t k = 0; k < nt; ++k) {
-        if (first + k < tile_cap) tiles[first + k] = make_uint2((uint32_t)v, k);
-        else raise_err(err, kDevOverflow);
-      }
-    }
+    warp_push_tiles((uint32_t)v, hv ? (uint32_t)((d + tile - 1) / tile) : 0u, tiles, &counts[0], tile_cap, err);
   }
 }
 
