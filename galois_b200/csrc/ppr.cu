@@ -54,6 +54,7 @@ struct PprState {
   float* wn_t = nullptr;  // [m] the same, transpose order
   uint32_t* flags = nullptr;  // [n/32] rows with a non-zero source term
   double* l1 = nullptr;       // [3][128] per-column L1 change ring
+  double* colnorm = nullptr;  // [128] per-column L1 norm of the adjoint's source term
   float* hacc = nullptr;      // [max(nheavy)][128]
   size_t hacc_rows = 0;
 };
@@ -71,6 +72,7 @@ void free_state(gb_graph* g) {
   cudaFree(st->wn_t);
   cudaFree(st->flags);
   cudaFree(st->l1);
+  cudaFree(st->colnorm);
   cudaFree(st->hacc);
   delete st;
   g->ppr_state = nullptr;
@@ -145,6 +147,7 @@ struct IterArgs {
   RowSched sched;
   float* hacc;  // [nheavy][128]
   double* l1;   // [3][128]
+  const double* col_scale;  // per-column stopping scale (nullptr: 1)
   IterCtl* ctl;
 };
 
@@ -292,10 +295,15 @@ __global__ void __launch_bounds__(kPprBlock) ppr_iterate(IterArgs a) {
     }
     __syncthreads();
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
-    double worst = 0.0;
-    for (uint32_t c = 0; c < a.B; ++c) worst = fmax(worst, *reinterpret_cast<volatile double*>(&a.l1[(it % 3) * 128 + c]));
+    // converged when every column's L1 change is at most tol (times the
+    // column's scale for the adjoint, whose source term is not normalised)
+    bool done = true;
+    for (uint32_t c = 0; c < a.B; ++c) {
+      const double lim = (double)a.tol * (a.col_scale ? a.col_scale[c] : 1.0);
+      done &= *reinterpret_cast<volatile double*>(&a.l1[(it % 3) * 128 + c]) <= lim;
+    }
     if (gtid == 0) ctl->iters = it + 1;
-    if (worst <= (double)a.tol || it + 1 >= a.max_iter) break;
+    if (done || it + 1 >= a.max_iter) break;
   }
 }
 
@@ -354,6 +362,23 @@ __global__ void __launch_bounds__(kPprBlock) ppr_grad_w(const uint64_t* __restri
   }
 }
 
+// out[c] = sum_r |src[r][c]| for the B columns of a vertex-major [n][B] array.
+__global__ void ppr_colnorm(const float* __restrict__ src, uint32_t n, uint32_t B, double* out) {
+  __shared__ double s_sum[128];
+  for (uint32_t c = threadIdx.x; c < 128; c += blockDim.x) s_sum[c] = 0.0;
+  __syncthreads();
+  const uint32_t rows_per_pass = blockDim.x / B;  // threads past rows_per_pass * B stay idle
+  const uint32_t c = threadIdx.x % B, r0 = threadIdx.x / B;
+  double acc = 0.0;
+  if (r0 < rows_per_pass)
+    for (uint64_t r = (uint64_t)blockIdx.x * rows_per_pass + r0; r < n; r += (uint64_t)gridDim.x * rows_per_pass)
+      acc += fabs((double)src[r * B + c]);
+  if (r0 < rows_per_pass) atomicAdd(&s_sum[c], acc);
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < B; k += blockDim.x)
+    if (s_sum[k] != 0.0) atomicAdd(&out[k], s_sum[k]);
+}
+
 __global__ void ppr_scale(const float* __restrict__ src, float scale, uint64_t count, float* __restrict__ dst) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -388,6 +413,7 @@ int ensure_state(gb_graph* g, cudaStream_t s, PprState** out) {
     GB_CUDA(cudaMalloc(&st->wn_t, sizeof(float) * std::max<uint64_t>(m, 1)));
     GB_CUDA(cudaMalloc(&st->flags, sizeof(uint32_t) * ((n + 31) / 32)));
     GB_CUDA(cudaMalloc(&st->l1, sizeof(double) * 3 * 128));
+    GB_CUDA(cudaMalloc(&st->colnorm, sizeof(double) * 128));
   }
   *out = static_cast<PprState*>(g->ppr_state);
   return GB_OK;
@@ -424,7 +450,14 @@ int solve(gb_graph* g, PprState* st, bool adjoint, uint32_t B, const float* src,
   a.max_iter = max_iter;
   a.hacc = st->hacc;
   a.l1 = st->l1;
+  a.col_scale = adjoint ? st->colnorm : nullptr;
   a.ctl = ctl;
+  if (adjoint) {
+    // the adjoint's source term (the loss gradient) has arbitrary scale: stop
+    // on the L1 change relative to each column's L1 norm
+    GB_CUDA(cudaMemsetAsync(st->colnorm, 0, sizeof(double) * 128, s));
+    ppr_colnorm<<<g->sm_count * 4, 256, 0, s>>>(src, g->n, B, st->colnorm);
+  }
   GB_CUDA(cudaMemsetAsync(ctl, 0, sizeof(IterCtl), s));
   GB_CUDA(cudaMemsetAsync(st->l1, 0, sizeof(double) * 3 * 128, s));
   GB_CUDA(cudaMemsetAsync(st->flags, 0, sizeof(uint32_t) * ((g->n + 31) / 32), s));

@@ -299,7 +299,9 @@ int gb_ppr_forward(gb_graph* g, uint32_t B, const float* teleport,
                    float* x_out, uint32_t* iters_out, gb_stats* stats,
                    void* stream);
 /* Adjoint of gb_ppr_forward: given x (forward solution) and gx = dL/dx, solves
- * lam = gx + alpha W~^T lam (Jacobi, same stopping rule) and returns
+ * lam = gx + alpha W~^T lam by Jacobi iteration until every column's L1
+ * change is <= tol times that column's L1 norm of gx (a loss gradient has no
+ * fixed scale, unlike a teleport distribution), and returns
  *   grad_teleport[n][B] = (1-alpha) lam
  *   grad_w[m]  = dL/dw_ji = alpha/s_j * sum_b x_j^b (lam_i^b - mu_j^b),
  *                mu_j = (lam_j - gx_j)/alpha, summed over the batch
