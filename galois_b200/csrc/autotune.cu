@@ -113,7 +113,7 @@ extern "C" int gb_autotune(gb_graph* g, const char* kernel, uint32_t src, const 
       t.heavy_degree = heavy;
       t.tile_edges = tile;
       if (k == "sssp") {
-        for (int depth : {-1, 2, 8}) {
+        for (int depth : {-1, 2, 8, 16}) {
           t.local_depth = depth;
           cands.push_back(t);
         }
