@@ -176,7 +176,9 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
         tile_fn(tv.x, tb, min(ve, tb + a.sched.tile));
       }
     }
-    if (__any_sync(kFull, my_change) && lane == 0) atomicOr(changed, 1u);
+    // read before the atomic: every warp changes something in the first sweep
+    if (__any_sync(kFull, my_change) && lane == 0 && *reinterpret_cast<volatile uint32_t*>(changed) == 0)
+      atomicOr(changed, 1u);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     compress_all(a, gtid, gthreads);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;

@@ -34,6 +34,11 @@ struct gb_graph {
   uint64_t* t_emap = nullptr;
   // cached per-graph derived arrays
   uint32_t* outdeg_of_stored = nullptr;  // PageRank nout (in-degree counts of the stored graph)
+  // degree-ordered graphs: row id of every arc of the light rows
+  // [lr_row0, zero_from), arcs [lr_arc0, lr_arc1), for flat pull sweeps
+  uint32_t* lr_rowid = nullptr;
+  uint32_t lr_row0 = 0, lr_heavy = 0;
+  uint64_t lr_arc0 = 0, lr_arc1 = 0;
   float* colsum = nullptr;               // PPR column sums of wf by source
   uint32_t max_degree = 0;
   // all-vertex sweep schedule (sweep.cuh), cached per (heavy, tile)

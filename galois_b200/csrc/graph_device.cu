@@ -267,7 +267,7 @@ int gb_graph_upload(const uint64_t* end_offs, const uint32_t* col, const uint32_
   if ((e = cudaMalloc(&g->col, sizeof(uint32_t) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc col"));
   if (w_u32 && (e = cudaMalloc(&g->w, sizeof(uint32_t) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc w"));
   if (w_f32 && (e = cudaMalloc(&g->wf, sizeof(float) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc wf"));
-  if ((e = cudaMallocHost(&g->pinned, 4096)) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
+  if ((e = cudaMallocHost(&g->pinned, 8192)) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
   cudaStream_t s = 0;
   if ((e = cudaMemsetAsync(g->offs, 0, sizeof(uint64_t), s)) != cudaSuccess) return fail(cuda_fail(e, "memset"));
   if ((e = cudaMemcpyAsync(g->offs + 1, end_offs, sizeof(uint64_t) * n, cudaMemcpyDefault, s)) != cudaSuccess) return fail(cuda_fail(e, "copy offs"));
@@ -319,6 +319,7 @@ int gb_graph_free(gb_graph* g) {
   cudaFree(g->t_wf);
   cudaFree(g->t_emap);
   cudaFree(g->outdeg_of_stored);
+  cudaFree(g->lr_rowid);
   cudaFree(g->colsum);
   if (g->ppr_free) g->ppr_free(g);
   cudaFree(g->sweep_tiles);

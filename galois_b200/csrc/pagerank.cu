@@ -39,13 +39,14 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kWarps = kBlock / 32;
+constexpr int kL1Slots = 32;  // the per-iteration L1 sum is spread over this many words
 
 struct PrCtl {
   GridBar bar;
   int err;
   uint32_t iters;
-  double l1[3];
-  uint32_t linf[3];  // max |delta| as float bits (non-negative floats order as uints)
+  double l1[3][kL1Slots];  // per-iteration L1 change, one slot per (CTA % kL1Slots)
+  uint32_t linf[3];        // max |delta| as float bits (non-negative floats order as uints)
   uint32_t active[3];
   uint32_t pad;
   FrontierCounters fc[3];
@@ -65,7 +66,11 @@ struct PrArgs {
   int linf;    // 1: stop on max |delta| (python/galois/_pagerank.pyx:114-139)
   float* value;
   float* c[2];
-  float* acc;
+  float* acc;   // per-row partial sums of heavy rows (and flat-swept light rows)
+  float* acc2;  // the alternate accumulator (pull kernels): iteration it adds into
+                // (it & 1 ? acc2 : acc) and zeroes the other; a plain store to a
+                // word the same iteration's atomics just updated stalled (~0.4 ms
+                // for 9 M words at RMAT-24), one iteration later it does not
   SweepSched sched;
   PrCtl* ctl;
   // residual variants
@@ -76,6 +81,10 @@ struct PrArgs {
   FrontierQueues fq;
   uint32_t heavy, tile;
   uint32_t zero_from;  // first vertex of the no-in-arc suffix (degree-ordered graphs), else n
+  // flat sweep of the light rows (degree-ordered graphs): arcs [lr_arc0, lr_arc1)
+  // with their row ids
+  const uint32_t* __restrict__ lr_rowid;
+  uint64_t lr_arc0, lr_arc1;
 };
 
 __global__ void count_nout(const uint32_t* __restrict__ col, uint64_t m, uint32_t* nout) {
@@ -93,6 +102,7 @@ __global__ void pr_pull_init(PrArgs a) {
     const uint32_t k = a.nout[v];
     a.c[0][v] = k ? init / (float)k : 0.f;
     a.acc[v] = 0.f;
+    a.acc2[v] = 0.f;
   }
 }
 
@@ -117,10 +127,64 @@ __device__ __forceinline__ bool seg_reduce(bool valid, uint32_t owner, float& x)
 // contributions sit on few lines and stay there.  On such a graph the
 // vertices from zero_from on have no in-arcs, so after two iterations their
 // rank and contribution are constants and their chunks are skipped.
+// Publish this thread's share of the iteration's L1 / max change: summed per
+// CTA in shared memory, then one atomic per CTA into one of kL1Slots words
+// (an atomic per warp on one word serialised ~7 K atomics per iteration), the
+// max with a read before the atomic.  All threads of the CTA call.
+__device__ __forceinline__ void publish_change(PrCtl* ctl, uint32_t slot_set, double my_l1, float my_max,
+                                               double* s_l1, uint32_t* s_max) {
+  my_l1 = warp_sum(my_l1);
+  const uint32_t mbits = __reduce_max_sync(kFull, __float_as_uint(my_max));
+  if (lane_id() == 0) {
+    if (my_l1 != 0.0) atomicAdd(s_l1, my_l1);
+    if (mbits != 0u) atomicMax(s_max, mbits);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (*s_l1 != 0.0) atomicAdd(&ctl->l1[slot_set][blockIdx.x % kL1Slots], *s_l1);
+    if (*s_max > *reinterpret_cast<volatile uint32_t*>(&ctl->linf[slot_set])) atomicMax(&ctl->linf[slot_set], *s_max);
+    *s_l1 = 0.0;
+    *s_max = 0u;
+  }
+}
+
+// The iteration's change after the barrier that follows publish_change: one
+// thread per CTA reads the slots and shares the total through shared memory
+// (every thread reading them would hammer the same L2 lines).  All threads
+// of the CTA call.
+__device__ __forceinline__ double read_change(const PrCtl* ctl, uint32_t slot_set, int linf, double* s_total) {
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    if (linf) {
+      v = (double)__uint_as_float(*reinterpret_cast<const volatile uint32_t*>(&ctl->linf[slot_set]));
+    } else {
+      for (int k = 0; k < kL1Slots; ++k) v += *reinterpret_cast<const volatile double*>(&ctl->l1[slot_set][k]);
+    }
+    *s_total = v;
+  }
+  __syncthreads();
+  const double v = *s_total;
+  __syncthreads();  // s_total is rewritten next iteration
+  return v;
+}
+
+// Zero the slots of iteration it+1 (by one thread, before that iteration's barrier).
+__device__ __forceinline__ void clear_change(PrCtl* ctl, uint32_t slot_set) {
+  for (int k = 0; k < kL1Slots; ++k) ctl->l1[slot_set][k] = 0.0;
+  ctl->linf[slot_set] = 0u;
+}
+
 template <int BLOCK, int U, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_persistent(PrArgs a) {
   constexpr int kW = BLOCK / 32;
   __shared__ float s_acc[kW][32];
+  __shared__ double s_l1, s_total;
+  __shared__ uint32_t s_max;
+  if (threadIdx.x == 0) {
+    s_l1 = 0.0;
+    s_max = 0u;
+  }
+  __syncthreads();
   PrCtl* ctl = a.ctl;
   const uint64_t deadline = kernel_deadline();
   const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
@@ -132,10 +196,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_persistent(PrArgs a) {
   for (uint32_t it = 0;; ++it) {
     const float* __restrict__ c_in = a.c[it & 1];
     float* __restrict__ c_out = a.c[(it + 1) & 1];
-    if (gtid == 0) {
-      ctl->l1[(it + 1) % 3] = 0.0;
-      ctl->linf[(it + 1) % 3] = 0u;
-    }
+    float* const acc_cur = (it & 1) ? a.acc2 : a.acc;
+    float* const acc_nxt = (it & 1) ? a.acc : a.acc2;
+    if (gtid == 0) clear_change(ctl, (it + 1) % 3);
     auto gather = [&](uint32_t u) -> float { return c_in[u]; };
     double my_l1 = 0.0;
     float my_max = 0.f;
@@ -210,26 +273,132 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_persistent(PrArgs a) {
           for (int k = 0; k < UT; ++k) u[k] = un[k];
         }
         sum = warp_sum(sum);
-        if (lane == 0) atomicAdd(&a.acc[tv.x], sum);
+        if (lane == 0) atomicAdd(&acc_cur[tv.x], sum);
       }
     }
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     for (uint64_t i = gtid; i < a.sched.nheavy; i += gthreads) {
       const uint32_t v = a.sched.heavy_list[i];
-      const float sum = a.acc[v];
-      a.acc[v] = 0.f;
+      const float sum = acc_cur[v];
+      acc_nxt[v] = 0.f;
       finish(v, sum);
     }
-    my_l1 = warp_sum(my_l1);
-    const uint32_t mbits = __reduce_max_sync(kFull, __float_as_uint(my_max));
-    if (lane == 0 && my_l1 != 0.0) atomicAdd(&ctl->l1[it % 3], my_l1);
-    if (lane == 0 && mbits != 0u) atomicMax(&ctl->linf[it % 3], mbits);
+    publish_change(ctl, it % 3, my_l1, my_max, &s_l1, &s_max);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
-    const double l1 = a.linf ? (double)__uint_as_float(*reinterpret_cast<volatile uint32_t*>(&ctl->linf[it % 3]))
-                             : *reinterpret_cast<volatile double*>(&ctl->l1[it % 3]);
+    const double l1 = read_change(ctl, it % 3, a.linf, &s_total);
     if (gtid == 0) ctl->iters = it + 1;
     if (l1 <= (double)a.tol || it + 1 >= a.max_iter) break;  // PageRank-pull.cpp:238-243
   }
+}
+
+// Jacobi pull iterations for a degree-ordered graph.  Its heavy rows are the
+// ids [0, nheavy) and its light rows follow with falling degree, so the light
+// rows' arcs form one contiguous range.  That range is swept flat, like a
+// tile: 256 arcs per warp task, 8 column ids and 8 row ids per lane loaded
+// together, 8 gathers in flight, a segmented warp sum per 32 arcs and one
+// atomicAdd per row segment into acc.  Heavy rows keep their tiles.  A
+// coalesced pass over the vertices then finishes every row from acc (rows
+// from zero_from on have no in-arcs: constant after two iterations, skipped).
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
+  __shared__ double s_l1, s_total;
+  __shared__ uint32_t s_max;
+  if (threadIdx.x == 0) {
+    s_l1 = 0.0;
+    s_max = 0u;
+  }
+  __syncthreads();
+  PrCtl* ctl = a.ctl;
+  const uint64_t deadline = kernel_deadline();
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const uint32_t lane = lane_id();
+  constexpr int UT = 8;
+  const uint64_t nruns = (a.lr_arc1 - a.lr_arc0 + 32 * UT - 1) / (32 * UT);
+  const uint64_t total = (uint64_t)a.sched.ntiles + nruns;
+  for (uint32_t it = 0;; ++it) {
+    const float* __restrict__ c_in = a.c[it & 1];
+    float* __restrict__ c_out = a.c[(it + 1) & 1];
+    float* const acc_cur = (it & 1) ? a.acc2 : a.acc;
+    float* const acc_nxt = (it & 1) ? a.acc : a.acc2;
+    if (gtid == 0) clear_change(ctl, (it + 1) % 3);
+    for (uint64_t t = gwarp; t < total; t += nwarps) {
+      if (t < a.sched.ntiles) {
+        // one tile of a heavy row (as in pr_pull_persistent)
+        const uint2 tv = a.sched.tiles[t];
+        const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
+        const uint64_t b = vb + (uint64_t)tv.y * a.sched.tile;
+        const uint64_t e = min(ve, b + a.sched.tile);
+        uint32_t u[UT];
+#pragma unroll
+        for (int k = 0; k < UT; ++k) {
+          const uint64_t i = b + lane + 32 * k;
+          u[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
+        }
+        float sum = 0.f;
+        for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
+          uint32_t un[UT];
+#pragma unroll
+          for (int k = 0; k < UT; ++k) {
+            const uint64_t i = i0 + 32 * UT + lane + 32 * k;
+            un[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
+          }
+#pragma unroll
+          for (int k = 0; k < UT; ++k) sum += u[k] != 0xFFFFFFFFu ? c_in[u[k]] : 0.f;
+#pragma unroll
+          for (int k = 0; k < UT; ++k) u[k] = un[k];
+        }
+        sum = warp_sum(sum);
+        if (lane == 0) atomicAdd(&acc_cur[tv.x], sum);
+      } else {
+        // 256 arcs of the light rows
+        const uint64_t r0 = a.lr_arc0 + (t - a.sched.ntiles) * (32 * UT);
+        uint32_t u[UT], row[UT];
+#pragma unroll
+        for (int k = 0; k < UT; ++k) {
+          const uint64_t i = r0 + lane + 32 * k;
+          const bool ok = i < a.lr_arc1;
+          u[k] = ok ? ldg(a.col + i) : 0u;
+          row[k] = ok ? ldg(a.lr_rowid + (i - a.lr_arc0)) : 0xFFFFFFFFu;
+        }
+        float x[UT];
+#pragma unroll
+        for (int k = 0; k < UT; ++k) x[k] = row[k] != 0xFFFFFFFFu ? c_in[u[k]] : 0.f;
+#pragma unroll
+        for (int k = 0; k < UT; ++k) {
+          if (seg_reduce(row[k] != 0xFFFFFFFFu, row[k], x[k])) atomicAdd(&acc_cur[row[k]], x[k]);
+        }
+      }
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    double my_l1 = 0.0;
+    float my_max = 0.f;
+    const uint32_t vend = it >= 2 ? a.zero_from : a.n;  // constant tail skipped
+    for (uint64_t v = gtid; v < vend; v += gthreads) {
+      const float sum = acc_cur[v];
+      acc_nxt[v] = 0.f;
+      const float value = sum * a.alpha + a.base;  // PageRank-pull.cpp:222
+      const float old = a.value[v];
+      a.value[v] = value;
+      const uint32_t k = a.nout[v];
+      c_out[v] = k ? value / (float)k : 0.f;
+      my_l1 += (double)fabsf(value - old);
+      my_max = fmaxf(my_max, fabsf(value - old));
+    }
+    publish_change(ctl, it % 3, my_l1, my_max, &s_l1, &s_max);
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    const double l1 = read_change(ctl, it % 3, a.linf, &s_total);
+    if (gtid == 0) ctl->iters = it + 1;
+    if (l1 <= (double)a.tol || it + 1 >= a.max_iter) break;  // PageRank-pull.cpp:238-243
+  }
+}
+
+__global__ void light_rowid_kernel(const uint64_t* __restrict__ offs, uint32_t row0, uint32_t row1, uint64_t arc0,
+                                   uint32_t* __restrict__ rowid) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = row0 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < row1; v += stride)
+    for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) rowid[e - arc0] = (uint32_t)v;
 }
 
 // ---- pull-residual (PageRank-pull.cpp:132-190) ------------------------------
@@ -445,6 +614,7 @@ inline float bits_to_float(uint32_t u) {
 int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_iter, float* rank_out,
                  uint32_t* iters_out, gb_stats* stats, cudaStream_t s, float init = -1.f, float base = -1.f,
                  int linf = 0) {
+  static_assert(sizeof(PrCtl) <= 4096, "PrCtl must fit the pinned readback area");
   if (!(alpha > 0.f && alpha < 1.f)) GB_FAIL(GB_ERR_ARG, "pagerank: alpha must be in (0,1)");
   if (!(tol >= 0.f)) GB_FAIL(GB_ERR_ARG, "pagerank: tolerance must be >= 0");
   if (max_iter == 0) GB_FAIL(GB_ERR_ARG, "pagerank: max_iter must be > 0");
@@ -460,7 +630,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
     if (st != GB_OK) return st;
   }
   FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
-  size_t need = carve_size<PrCtl>(1) + 4 * carve_size<float>(n) + (out_dev ? 0 : carve_size<float>(n));
+  size_t need = carve_size<PrCtl>(1) + 5 * carve_size<float>(n) + (out_dev ? 0 : carve_size<float>(n));
   if (kind != PrKind::Pull) need += 2 * carve_size<float>(n);
   if (kind == PrKind::Push) need += 3 * carve_size<uint32_t>(n) + fl.bytes;
   st = ws_reserve(g, need, s);
@@ -471,6 +641,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
   a.c[0] = cv.take<float>(n);
   a.c[1] = cv.take<float>(n);
   a.acc = cv.take<float>(n);
+  a.acc2 = cv.take<float>(n);
   if (kind != PrKind::Pull) {
     a.residual = cv.take<float>(n);
     a.delta = cv.take<float>(n);
@@ -501,6 +672,31 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
     pr_pull_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     a.zero_from = g->perm ? g->zero_from : n;
     kfn = reinterpret_cast<const void*>(&pr_pull_persistent<kBlock, 2, 6>);
+    if (g->perm) {
+      // degree-ordered: heavy rows are [0, nheavy), the light rows' arcs one
+      // contiguous range; their row ids are built once per heavy threshold
+      if (!g->lr_rowid || g->lr_heavy != sched.heavy) {
+        cudaFree(g->lr_rowid);
+        g->lr_rowid = nullptr;
+        uint64_t ends[2] = {0, 0};
+        GB_CUDA(cudaMemcpyAsync(&ends[0], g->offs + sched.nheavy, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaMemcpyAsync(&ends[1], g->offs + g->zero_from, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaStreamSynchronize(s));
+        if (ends[1] < ends[0]) GB_FAIL(GB_ERR_CUDA, "pagerank: light rows out of order");
+        GB_CUDA(cudaMalloc(&g->lr_rowid, sizeof(uint32_t) * std::max<uint64_t>(ends[1] - ends[0], 1)));
+        if (g->zero_from > sched.nheavy)
+          light_rowid_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, sched.nheavy, g->zero_from, ends[0], g->lr_rowid);
+        GB_CUDA(cudaGetLastError());
+        g->lr_row0 = sched.nheavy;
+        g->lr_heavy = sched.heavy;
+        g->lr_arc0 = ends[0];
+        g->lr_arc1 = ends[1];
+      }
+      a.lr_rowid = g->lr_rowid;
+      a.lr_arc0 = g->lr_arc0;
+      a.lr_arc1 = g->lr_arc1;
+      kfn = reinterpret_cast<const void*>(&pr_pull_flat<kBlock, 6>);
+    }
   } else if (kind == PrKind::PullResidual) {
     pr_resid_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     GB_CUDA(cudaMemsetAsync(a.acc, 0, sizeof(float) * n, s));
@@ -516,7 +712,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
   KernelTimer kt(stats != nullptr, s);
   GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, kBlock, args, 0, s));
   kt.stop(s);
-  PrCtl* hc = reinterpret_cast<PrCtl*>(static_cast<char*>(g->pinned) + 256);
+  PrCtl* hc = reinterpret_cast<PrCtl*>(static_cast<char*>(g->pinned) + 4096);  // PrCtl is ~1 KB
   GB_CUDA(cudaMemcpyAsync(hc, a.ctl, sizeof(PrCtl), cudaMemcpyDeviceToHost, s));
   if (!out_dev) {
     st = copy_out(rank_out, a.value, sizeof(float) * n, s);
@@ -534,8 +730,9 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
       stats->relaxations = hc->pushes;
       stats->launches = 2;
       stats->kernel_ms = kt.ms();
-      stats->residual = kind == PrKind::Pull ? (linf ? (double)bits_to_float(hc->linf[(hc->iters + 2) % 3])
-                                                     : hc->l1[(hc->iters + 2) % 3])
+      double l1sum = 0.0;
+      for (int k = 0; k < kL1Slots; ++k) l1sum += hc->l1[(hc->iters + 2) % 3][k];
+      stats->residual = kind == PrKind::Pull ? (linf ? (double)bits_to_float(hc->linf[(hc->iters + 2) % 3]) : l1sum)
                                              : 0.0;
     }
     if (kind != PrKind::Push && hc->iters >= max_iter) {

@@ -135,6 +135,8 @@ void drop_derived(gb_graph* g) {
   g->t_wf = nullptr;
   g->t_emap = nullptr;
   cudaFree(g->outdeg_of_stored);
+  cudaFree(g->lr_rowid);
+  g->lr_rowid = nullptr;
   cudaFree(g->colsum);
   g->outdeg_of_stored = nullptr;
   g->colsum = nullptr;
