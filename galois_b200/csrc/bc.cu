@@ -66,7 +66,9 @@ struct MsArgs {
   double* sigma;              // [n][64]
   float* dep;                 // [n][64]
   double* bc;                 // [n]
-  double* hacc;               // [nheavy][64] backward partial sums of heavy vertices
+  double* hacc;               // [2][nheavy][64] backward partial sums of heavy vertices; level L adds
+                              // into half L & 1 and zeroes the other half (a store to a word this
+                              // level's atomics just updated stalls)
   uint32_t* hidx;             // [n] heavy-list index of a heavy vertex
   SweepSched fs;              // heavy schedule over in-edges (forward)
   SweepSched bs;              // heavy schedule over out-edges (backward)
@@ -86,7 +88,7 @@ __global__ void ms_init(MsArgs a) {
   }
   for (uint64_t i = tid; i < (uint64_t)a.lcap * a.n; i += stride) a.lm[i] = 0ull;
   for (uint64_t v = tid; v < a.n; v += stride) a.visit[v] = 0ull;
-  for (uint64_t i = tid; i < (uint64_t)a.bs.nheavy * 64; i += stride) a.hacc[i] = 0.0;
+  for (uint64_t i = tid; i < 2ull * a.bs.nheavy * 64; i += stride) a.hacc[i] = 0.0;
   for (uint64_t i = tid; i < a.bs.nheavy; i += stride) a.hidx[a.bs.heavy_list[i]] = (uint32_t)i;
 }
 
@@ -248,6 +250,8 @@ __global__ void __launch_bounds__(kBcBlock) ms_persistent(MsArgs a) {
   for (int Lb = (int)nlev - 2; Lb >= 1; --Lb) {
     const unsigned long long* cur = a.lm + (uint64_t)Lb * a.n;
     const unsigned long long* nextl = a.lm + (uint64_t)(Lb + 1) * a.n;
+    double* const hcur = a.hacc + (uint64_t)(Lb & 1) * a.bs.nheavy * 64;
+    double* const hoth = a.hacc + (uint64_t)((Lb + 1) & 1) * a.bs.nheavy * 64;
     ms_for_light(a, a.bs, a.offs, gwarp, nwarps, [&](uint32_t v, bool light) {
       const unsigned long long cv = light ? cur[v] : 0ull;
       unsigned sel = __ballot_sync(kFull, cv != 0);
@@ -282,27 +286,32 @@ __global__ void __launch_bounds__(kBcBlock) ms_persistent(MsArgs a) {
       const uint64_t b = vb + (uint64_t)tv.y * a.bs.tile, e = min(ve, b + a.bs.tile);
       double dA = 0.0, dB = 0.0;
       ms_backward_range(a, nextl, cv, b, e, dA, dB);
-      double* h = a.hacc + (uint64_t)a.hidx[tv.x] * 64;
+      double* h = hcur + (uint64_t)a.hidx[tv.x] * 64;
       if ((cv >> lane) & 1ull) atomicAdd(&h[lane], dA);
       if ((cv >> (lane + 32)) & 1ull) atomicAdd(&h[lane + 32], dB);
     }
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     for (uint64_t i = gwarp; i < a.bs.nheavy; i += nwarps) {
       const uint32_t v = a.bs.heavy_list[i];
+      // clear what level Lb+1 left in the other half (level Lb-1 adds there)
+      const unsigned long long prev = nextl[v];
+      if (prev) {
+        double* ho = hoth + i * 64;
+        if ((prev >> lane) & 1ull) ho[lane] = 0.0;
+        if ((prev >> (lane + 32)) & 1ull) ho[lane + 32] = 0.0;
+      }
       const unsigned long long cv = cur[v];
       if (!cv) continue;
-      double* h = a.hacc + i * 64;
+      const double* h = hcur + i * 64;
       const uint64_t r = (uint64_t)v * 64;
       double t = 0.0;
       if ((cv >> lane) & 1ull) {
         const float d = (float)(h[lane] * a.sigma[r + lane]);
-        h[lane] = 0.0;
         a.dep[r + lane] = d;
         t += d;
       }
       if ((cv >> (lane + 32)) & 1ull) {
         const float d = (float)(h[lane + 32] * a.sigma[r + lane + 32]);
-        h[lane + 32] = 0.0;
         a.dep[r + lane + 32] = d;
         t += d;
       }
@@ -596,7 +605,7 @@ int run_bc(gb_graph* g, const uint32_t* srcs_in, uint32_t nsrc, uint32_t batch, 
     for (int attempt = 0;; ++attempt) {
       const size_t need = carve_size<BcCtl>(1) + carve_size<double>(n) + carve_size<unsigned long long>((size_t)lcap * n) +
                           carve_size<unsigned long long>(n) + carve_size<double>((size_t)n * 64) +
-                          carve_size<float>((size_t)n * 64) + carve_size<double>((size_t)sched.nheavy * 64 + 1) +
+                          carve_size<float>((size_t)n * 64) + carve_size<double>(2 * (size_t)sched.nheavy * 64 + 1) +
                           carve_size<uint32_t>(n) + carve_size<uint32_t>(64) + (out_dev ? 0 : carve_size<float>(n));
       st = ws_reserve(g, need, s);
       if (st != GB_OK) return st;
@@ -609,7 +618,7 @@ int run_bc(gb_graph* g, const uint32_t* srcs_in, uint32_t nsrc, uint32_t batch, 
       a.visit = cv.take<unsigned long long>(n);
       a.sigma = cv.take<double>((size_t)n * 64);
       a.dep = cv.take<float>((size_t)n * 64);
-      a.hacc = cv.take<double>((size_t)sched.nheavy * 64 + 1);
+      a.hacc = cv.take<double>(2 * (size_t)sched.nheavy * 64 + 1);
       a.hidx = cv.take<uint32_t>(n);
       uint32_t* dsrc = cv.take<uint32_t>(64);
       out32 = out_dev ? bc_out : cv.take<float>(n);
