@@ -113,6 +113,7 @@ SIGNATURES: dict[str, tuple] = {
                                          C.POINTER(_vp)]),
     "gb_graph_build_transpose": (C.c_int, [_gp, _vp]),
     "gb_graph_reorder": (C.c_int, [_gp, C.c_int, _vp]),
+    "gb_pool_trim": (C.c_int, []),
     "gb_graph_permutation": (C.c_int, [_gp, C.POINTER(_vp), C.POINTER(_vp)]),
     "gb_graph_set_tuning": (C.c_int, [_gp, C.POINTER(Tuning)]),
     "gb_graph_get_tuning": (C.c_int, [_gp, C.POINTER(Tuning)]),

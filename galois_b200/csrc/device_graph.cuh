@@ -88,6 +88,18 @@ int cuda_fail(cudaError_t e, const char* what);
   } while (0)
 
 bool is_device_ptr(const void* p);
+
+// Caching allocator for the large per-graph arrays (CSR mirror, workspace)
+// and the pinned readback buffer: blocks freed by gb_graph_free are kept,
+// keyed by device and size rounded to 2 MiB, and handed to the next upload of
+// the same shape, so a repeated upload/compute/free cycle makes no
+// cudaMalloc / cudaFree (each of which can cost milliseconds and cudaFree
+// synchronises the device).  pool_free accepts memory from cudaMalloc too.
+// gb_pool_trim (gb.h) releases the cached blocks.
+cudaError_t pool_malloc(void** p, size_t bytes);
+void pool_free(void* p);
+cudaError_t pool_malloc_host(void** p, size_t bytes);
+void pool_free_host(void* p);
 // Ensure at least `bytes` of workspace; returns GB_OK or an error status.
 int ws_reserve(gb_graph* g, size_t bytes, cudaStream_t stream);
 // Bump-carve helper over the workspace.

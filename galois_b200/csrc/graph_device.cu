@@ -10,6 +10,10 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
 
 #include "device_common.cuh"
 #include "device_graph.cuh"
@@ -33,21 +37,98 @@ bool is_device_ptr(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+namespace {
+
+struct Pool {
+  std::mutex mu;
+  // (device, rounded size) -> cached blocks; -1 is the pinned-host pool
+  std::map<std::pair<int, size_t>, std::vector<void*>> free_blocks;
+  std::unordered_map<void*, std::pair<int, size_t>> live;
+};
+
+Pool& pool() {
+  static Pool* p = new Pool();  // never destroyed: blocks may be freed during process exit
+  return *p;
+}
+
+size_t pool_round(size_t bytes) {
+  const size_t g = bytes > (1u << 20) ? (2u << 20) : 4096;
+  return (std::max<size_t>(bytes, 1) + g - 1) / g * g;
+}
+
+void pool_trim_locked(Pool& P, int device) {
+  for (auto it = P.free_blocks.begin(); it != P.free_blocks.end();) {
+    if (device == -2 || it->first.first == device) {
+      for (void* b : it->second) {
+        if (it->first.first == -1) cudaFreeHost(b);
+        else cudaFree(b);
+      }
+      it = P.free_blocks.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+cudaError_t pool_get(void** p, size_t bytes, bool host) {
+  int dev = -1;
+  if (!host && cudaGetDevice(&dev) != cudaSuccess) return cudaErrorInvalidDevice;
+  const size_t sz = pool_round(bytes);
+  Pool& P = pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  auto it = P.free_blocks.find({dev, sz});
+  if (it != P.free_blocks.end() && !it->second.empty()) {
+    *p = it->second.back();
+    it->second.pop_back();
+    P.live[*p] = {dev, sz};
+    return cudaSuccess;
+  }
+  cudaError_t e = host ? cudaMallocHost(p, sz) : cudaMalloc(p, sz);
+  if (e != cudaSuccess) {  // give the cached blocks of this device back and retry
+    cudaGetLastError();
+    pool_trim_locked(P, dev);
+    e = host ? cudaMallocHost(p, sz) : cudaMalloc(p, sz);
+  }
+  if (e == cudaSuccess) P.live[*p] = {dev, sz};
+  return e;
+}
+
+void pool_put(void* p, bool host) {
+  if (!p) return;
+  Pool& P = pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  auto it = P.live.find(p);
+  if (it == P.live.end()) {  // not from the pool
+    if (host) cudaFreeHost(p);
+    else cudaFree(p);
+    return;
+  }
+  P.free_blocks[it->second].push_back(p);
+  P.live.erase(it);
+}
+
+}  // namespace
+
+cudaError_t pool_malloc(void** p, size_t bytes) { return pool_get(p, bytes, false); }
+void pool_free(void* p) { pool_put(p, false); }
+cudaError_t pool_malloc_host(void** p, size_t bytes) { return pool_get(p, bytes, true); }
+void pool_free_host(void* p) { pool_put(p, true); }
+
 int ws_reserve(gb_graph* g, size_t bytes, cudaStream_t stream) {
   if (bytes <= g->ws_bytes) return GB_OK;
   if (g->ws) {
     GB_CUDA(cudaStreamSynchronize(stream));
-    GB_CUDA(cudaFree(g->ws));
+    pool_free(g->ws);
     g->ws = nullptr;
     g->ws_bytes = 0;
   }
   size_t want = bytes + bytes / 8;  // headroom so repeat calls do not regrow
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, want);
+  cudaError_t e = pool_malloc(&p, want);
   if (e != cudaSuccess) {
     cudaGetLastError();
     want = bytes;
-    GB_CUDA(cudaMalloc(&p, want));
+    GB_CUDA(pool_malloc(&p, want));
   }
   g->ws = p;
   g->ws_bytes = want;
@@ -263,11 +344,12 @@ int gb_graph_upload(const uint64_t* end_offs, const uint32_t* col, const uint32_
     return st;
   };
   cudaError_t e;
-  if ((e = cudaMalloc(&g->offs, sizeof(uint64_t) * (n + 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc offs"));
-  if ((e = cudaMalloc(&g->col, sizeof(uint32_t) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc col"));
-  if (w_u32 && (e = cudaMalloc(&g->w, sizeof(uint32_t) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc w"));
-  if (w_f32 && (e = cudaMalloc(&g->wf, sizeof(float) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc wf"));
-  if ((e = cudaMallocHost(&g->pinned, 8192)) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
+  auto dalloc = [](auto** p, size_t bytes) { return pool_malloc(reinterpret_cast<void**>(p), bytes); };
+  if ((e = dalloc(&g->offs, sizeof(uint64_t) * (n + 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc offs"));
+  if ((e = dalloc(&g->col, sizeof(uint32_t) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc col"));
+  if (w_u32 && (e = dalloc(&g->w, sizeof(uint32_t) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc w"));
+  if (w_f32 && (e = dalloc(&g->wf, sizeof(float) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc wf"));
+  if ((e = pool_malloc_host(&g->pinned, 8192)) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
   cudaStream_t s = 0;
   if ((e = cudaMemsetAsync(g->offs, 0, sizeof(uint64_t), s)) != cudaSuccess) return fail(cuda_fail(e, "memset"));
   if ((e = cudaMemcpyAsync(g->offs + 1, end_offs, sizeof(uint64_t) * n, cudaMemcpyDefault, s)) != cudaSuccess) return fail(cuda_fail(e, "copy offs"));
@@ -277,14 +359,14 @@ int gb_graph_upload(const uint64_t* end_offs, const uint32_t* col, const uint32_
   int* flag = static_cast<int*>(g->pinned);
   unsigned* maxdeg = reinterpret_cast<unsigned*>(static_cast<char*>(g->pinned) + 64);
   int* dflag = nullptr;
-  if ((e = cudaMalloc(&dflag, 64)) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc flag"));
+  if ((e = pool_malloc(reinterpret_cast<void**>(&dflag), 64)) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc flag"));
   cudaMemsetAsync(dflag, 0, 64, s);
   validate_kernel<<<g->sm_count * 4, 256, 0, s>>>(g->offs, g->col, n, m, dflag);
   degree_max_kernel<<<g->sm_count * 4, 256, 0, s>>>(g->offs, n, reinterpret_cast<unsigned*>(dflag + 4));
   cudaMemcpyAsync(flag, dflag, 4, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(maxdeg, dflag + 4, 4, cudaMemcpyDeviceToHost, s);
   e = cudaStreamSynchronize(s);
-  cudaFree(dflag);
+  pool_free(dflag);
   if (e != cudaSuccess) return fail(cuda_fail(e, "graph validation"));
   if (*flag) {
     gb_graph_free(g);
@@ -310,10 +392,12 @@ int gb_graph_load_gr(const char* path, int edge_bytes, int symmetric, int device
 int gb_graph_free(gb_graph* g) {
   if (!g) return GB_OK;
   cudaSetDevice(g->device);
-  cudaFree(g->offs);
-  cudaFree(g->col);
-  cudaFree(g->w);
-  cudaFree(g->wf);
+  // pooled blocks are reused by the next upload: no kernel may still use them
+  cudaDeviceSynchronize();
+  pool_free(g->offs);
+  pool_free(g->col);
+  pool_free(g->w);
+  pool_free(g->wf);
   cudaFree(g->t_offs);
   cudaFree(g->t_col);
   cudaFree(g->t_wf);
@@ -333,9 +417,17 @@ int gb_graph_free(gb_graph* g) {
   cudaFree(g->iperm);
   cudaFree(g->ro_buf);
   std::free(g->h_iperm);
-  cudaFree(g->ws);
-  if (g->pinned) cudaFreeHost(g->pinned);
+  pool_free(g->ws);
+  pool_free_host(g->pinned);
   delete g;
+  return GB_OK;
+}
+
+int gb_pool_trim(void) {
+  clear_error();
+  Pool& P = pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  pool_trim_locked(P, -2);
   return GB_OK;
 }
 

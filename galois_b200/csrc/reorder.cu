@@ -331,10 +331,10 @@ int reorder_graph(gb_graph* g, int order, cudaStream_t s) {
 
   // install
   drop_derived(g);
-  cudaFree(g->offs);
-  cudaFree(g->col);
-  cudaFree(g->w);
-  cudaFree(g->wf);
+  pool_free(g->offs);
+  pool_free(g->col);
+  pool_free(g->w);
+  pool_free(g->wf);
   g->offs = noffs;
   g->col = ncol;
   g->w = nw;

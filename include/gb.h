@@ -137,6 +137,10 @@ int gb_graph_upload(const uint64_t* end_offs, const uint32_t* col,
 int gb_graph_load_gr(const char* path, int edge_bytes, int symmetric,
                      int device, gb_graph** out);
 int gb_graph_free(gb_graph* g);
+/* gb_graph_free keeps the graph's large device blocks (and its pinned
+ * readback buffer) in a process-wide cache for the next upload of the same
+ * shape; this releases every cached block. */
+int gb_pool_trim(void);
 int gb_graph_info(const gb_graph* g, uint32_t* n, uint64_t* m,
                   int* symmetric);
 /* Device-resident begin offsets (n+1), columns and weights (NULL if absent):
