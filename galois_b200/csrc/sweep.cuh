@@ -63,37 +63,4 @@ __device__ __forceinline__ void sweep_all(const uint64_t* __restrict__ offs, uin
   }
 }
 
-// sweep_all with U steps of memory loads in flight per lane (warp_expand_mlp)
-// for the light vertices; heavy tiles as in sweep_all.
-template <int U, class T, class Load1, class Load2, class Consume, class ChunkDoneFn, class TileFn>
-__device__ __forceinline__ void sweep_all_mlp(const uint64_t* __restrict__ offs, uint32_t n, const SweepSched& s,
-                                              uint64_t gwarp, uint64_t nwarps, Load1&& load1, Load2&& load2,
-                                              Consume&& consume, ChunkDoneFn&& chunk_done, TileFn&& tile_fn) {
-  const uint32_t lane = lane_id();
-  const uint64_t nchunks = ((uint64_t)n + 31) >> 5;
-  const uint64_t total = nchunks + s.ntiles;
-  for (uint64_t t = gwarp; t < total; t += nwarps) {
-    if (t < nchunks) {
-      const uint64_t v = (t << 5) + lane;
-      uint64_t b = 0;
-      uint32_t d = 0;
-      bool heavy = false;
-      if (v < n) {
-        b = ldg(offs + v);
-        const uint64_t dd = ldg(offs + v + 1) - b;
-        heavy = dd > s.heavy;
-        d = heavy ? 0u : (uint32_t)dd;
-      }
-      warp_expand_mlp<U, T>(b, d, (uint32_t)v, load1, load2, consume);
-      chunk_done((uint32_t)v, v < n, heavy);
-    } else {
-      const uint2 tv = s.tiles[t - nchunks];
-      const uint64_t vb = ldg(offs + tv.x), ve = ldg(offs + tv.x + 1);
-      const uint64_t b = vb + (uint64_t)tv.y * s.tile;
-      const uint64_t e = min(ve, b + s.tile);
-      tile_fn(tv.x, b, e);
-    }
-  }
-}
-
 }  // namespace gb
