@@ -214,18 +214,26 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
       };
       const uint32_t* qin = a.fq.light[P & 1];
       const uint2* tin = a.fq.tiles[P & 1];
+      // A large frontier is swept densely: every vertex in id order, active
+      // when its stamp names this phase (it was queued for it and not queued
+      // again since; a vertex re-queued for the next phase is expanded there
+      // with its newer distance).  Consecutive rows keep the column and
+      // weight reads contiguous, which the queue's arbitrary order does not.
+      const bool dense = q_light > (a.n >> 4);
+      const uint32_t nl = dense ? a.n : q_light;
       for_each_frontier_task(
-          q_light, q_tiles, gwarp, nwarps,
+          nl, q_tiles, gwarp, nwarps,
           [&](uint32_t base, uint32_t vpt) {
             const uint32_t idx = base + lane;
-            const bool has = lane < vpt && idx < q_light;
+            const bool has = lane < vpt && idx < nl;
             uint64_t b = 0;
             uint32_t d = 0, dv = 0;
             if (has) {
-              const uint32_t v = qin[idx];
+              const uint32_t v = dense ? idx : qin[idx];
               b = ldg(a.offs + v);
               d = (uint32_t)(ldg(a.offs + v + 1) - b);
               dv = __ldcg(a.dist + v);
+              if (dense && (a.stamp[v] != P || d > a.heavy)) d = 0;  // not this phase's light vertex
             }
             expand(b, d, dv, dv, true);
           },
