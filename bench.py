@@ -96,6 +96,16 @@ class Dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
     def close(self):
         if self.pg:
             import torch.distributed as dist
@@ -566,6 +576,58 @@ def run_batched(args) -> None:
     emit(line)
 
 
+def run_bc_sharded(args) -> None:
+    """--app bc on N GPUs: the 1024 sources are sharded over the ranks and one
+    NCCL all-reduce sums the partial centralities (strong scaling: the total
+    work is fixed)."""
+    import torch
+
+    from galois_b200 import DeviceGraph, rmat
+    from galois_b200.distributed import bc_sharded, shard_sources
+
+    dist = Dist(want_pg=True)
+    dev = dist.local_rank
+    torch.cuda.set_device(dev)
+    scale = pick(args.size, 14, 17, 20)
+    g, _ = rmat(scale, 16, seed=20, symmetrize=True)
+    rng = np.random.default_rng(1024)
+    srcs = rng.choice(np.flatnonzero(g.degrees() > 0), 1024, replace=False).astype(np.uint32)
+    dg = DeviceGraph(g, symmetric=True, device=dev)
+    lv = torch.empty(g.n, dtype=torch.int32, device=f"cuda:{dev}")
+    mine = shard_sources(srcs, dist.rank, dist.world)
+    m_r_mine = float(sum(dg.bfs(int(s), out=lv, stats=True)[1]["edges_reached"] for s in mine))
+    units = 2.0 * dist.sum(m_r_mine)  # forward + backward arcs of all sources, whole job
+    out = torch.empty(g.n, dtype=torch.float32, device=f"cuda:{dev}")
+    for _ in range(max(args.warmup, 1)):
+        bc_sharded(dg, srcs, out, 64)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        bc_sharded(dg, srcs, out, 64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    t_ms = dist.max(e0.elapsed_time(e1))
+    if dist.rank == 0:
+        emit({"metric": "BC aggregate GTEPS (fwd+bwd arcs of reached vertices, 1024 sources)", "unit": "GTEPS",
+              "value": units * args.steps / (t_ms / 1e3) / 1e9, "n_gpus": dist.world, "steps": args.steps,
+              "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+              "scaling": "strong", "vs_baseline": None, "dtype": "f64 sigma / f32 dependency",
+              "data": "synthetic (seeded generators)",
+              "config": {"workload": f"Brandes BC, RMAT-{scale} sym ef16, 1024 seeded sources sharded over "
+                                     f"{dist.world} GPUs, 64 per launch, one all-reduce of bc per step",
+                         "n": g.n, "m": g.m, "parallelism": f"sources/{dist.world}"},
+              "clocks": clk, "gpu_launches": (3 * (len(mine) // 64) + 2) * args.steps})
+    dg.free()
+    dist.close()
+
+
 def cpu_units(job: Job, gpu_stats: list) -> float:
     return sum(job.units(st, gi) for gi, st in enumerate(gpu_stats))
 
@@ -624,7 +686,9 @@ def main() -> None:
                 emit({"impl": "reference", "unavailable": f"--app {args.app}: the CPU baseline is reported inside the "
                                                           "GPU line (cpu_baseline); see the default SSSP workload"})
             return
-        if rank == 0:
+        if args.app == "bc" and int(os.environ.get("WORLD_SIZE", "1")) > 1:
+            run_bc_sharded(args)  # every rank: sources sharded, one all-reduce
+        elif rank == 0:
             run_batched(args)
         return
     job_cls = JOBS[args.app]

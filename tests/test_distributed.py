@@ -1,8 +1,9 @@
-"""Multi-process plumbing of bench.py on CPU: two gloo ranks run the same
-barrier / max-over-ranks timing path the NCCL ranks take, and the whole-job
-rate is the units of all ranks over the slowest rank's time.  The multi-GPU
-path has no data exchange (every rank runs its own replica of the workload),
-so these host-side steps are all of it."""
+"""Multi-process plumbing on CPU: two gloo ranks run the same barrier /
+max-over-ranks timing path the NCCL ranks of bench.py take (the whole-job
+rate is the units of all ranks over the slowest rank's time), and the
+source-sharded BC (galois_b200.distributed) splits the sources without gaps
+or overlap and sums the partial centralities with one all-reduce.  Every
+other kernel runs one replica per GPU, with no data exchange."""
 import importlib.util
 import os
 import socket
@@ -42,7 +43,8 @@ def _rank_main(rank, world, port, q):
         local = (time.perf_counter() - t0) * 1e3
         got = d.max(float(10 * (rank + 1)))
         wall = d.max(local)
-        q.put((rank, d.world, got, wall, local))
+        total = d.sum(float(rank + 1))
+        q.put((rank, d.world, got, wall, local, total))
     finally:
         d.close()
 
@@ -61,6 +63,7 @@ def test_dist_gloo_world2_max_and_barrier():
     res.sort()
     assert [r[1] for r in res] == [2, 2]
     assert all(r[2] == 20.0 for r in res)  # max over ranks, on every rank
+    assert all(r[5] == 3.0 for r in res)  # sum over ranks, on every rank
     walls = {round(r[3], 9) for r in res}
     assert len(walls) == 1  # both ranks agree on one job time
     assert res[0][3] >= max(r[4] for r in res) - 1e-9
@@ -76,6 +79,78 @@ def test_dist_single_process_is_noop(monkeypatch):
     d.barrier()
     assert d.max(3.5) == 3.5
     d.close()
+
+
+class _FakeBcGraph:
+    """Stands in for a DeviceGraph: source s contributes (1 + s) at vertex s
+    and 1 at vertex 0, so the reduced vector identifies every source."""
+
+    def __init__(self, n):
+        self.n = n
+        self.calls = []
+
+    def bc(self, sources, batch, out):
+        self.calls.append(list(map(int, sources)))
+        out.zero_()
+        for s in sources:
+            out[int(s)] += 1.0 + float(s)
+            out[0] += 1.0
+
+
+def _bc_rank(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from galois_b200.distributed import bc_sharded
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        n = 40
+        sources = [3, 7, 11, 12, 20, 31, 33]
+        g = _FakeBcGraph(n)
+        out = torch.empty(n, dtype=torch.float32)
+        bc_sharded(g, sources, out, batch=64)
+        q.put((rank, g.calls, out.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bc_sources_sharded_and_reduced():
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_bc_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    sources = [3, 7, 11, 12, 20, 31, 33]
+    owned = [c for r in res for call in r[1] for c in call]
+    assert sorted(owned) == sources  # every source exactly once
+    assert all(len(r[1]) == 1 for r in res)  # one bc call per rank
+    want = [0.0] * 40
+    for s in sources:
+        want[s] += 1.0 + s
+    want[0] += len(sources)
+    for r in res:
+        assert r[2] == want  # every rank holds the full sum
+
+
+def test_shard_sources_edges():
+    from galois_b200.distributed import shard_sources
+
+    src = list(range(10))
+    parts = [shard_sources(src, r, 3).tolist() for r in range(3)]
+    assert sorted(sum(parts, [])) == src
+    assert shard_sources([], 0, 4).size == 0
+    assert shard_sources(src, 3, 4).tolist() == [3, 7]  # more ranks than sources in a stride
+    with pytest.raises(ValueError):
+        shard_sources(src, 2, 2)
 
 
 @pytest.mark.parametrize("world", [1, 2, 4, 8])

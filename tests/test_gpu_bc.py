@@ -68,3 +68,33 @@ def test_bc_directed_single_source_and_errors(cuda_device):
         assert e.value.status == _lib.GB_ERR_UNSUPPORTED
         with pytest.raises(GbError):
             dg.bc([g.n], batch=1)
+
+
+def test_bc_sharded_single_rank_matches_plain(cuda_device):
+    """galois_b200.distributed over a one-rank NCCL group equals plain gb_bc
+    (the multi-rank split and sum are covered by the gloo tests)."""
+    import datetime
+    import os
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from galois_b200.distributed import bc_sharded
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    try:
+        g, _ = rmat(11, 8, seed=44)
+        srcs = np.random.default_rng(5).choice(g.n, 100, replace=False).astype(np.uint32)
+        with DeviceGraph(g, symmetric=True) as dg:
+            want = dg.bc(srcs, batch=64)
+            out = torch.empty(g.n, dtype=torch.float32, device="cuda")
+            bc_sharded(dg, srcs, out, batch=64)
+            assert np.abs(out.cpu().numpy() - want).max() <= 1e-6 * max(1.0, float(np.abs(want).max()))
+    finally:
+        dist.destroy_process_group()
