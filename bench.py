@@ -745,7 +745,9 @@ def main() -> None:
     peak, peak_src = measured_peak_hbm()
     achieved = bytes_step / (sum(kms) / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_src, "kernel": job.kernel,
+                "peak_source": peak_src,
+                # a degree-ordered PageRank runs the flat pull kernel
+                "kernel": "pr_pull_flat" if (isinstance(job, PrJob) and args.order) else job.kernel,
                 "algorithmic_bytes_per_step": bytes_step, "kernel_ms_per_step": sum(kms),
                 "traffic": traffic_from_profiles(f"{args.app}-{args.size}")}
     line = {"metric": job.metric, "value": value, "unit": job.unit, "n_gpus": dist.world, "steps": args.steps,
