@@ -74,3 +74,25 @@ def test_load_gr_and_autotune(cuda_device, gr_files, tmp_path):
         assert (dg.cc() == oracle.cc_union_find(g)).all()
     finally:
         dg.free()
+
+
+def test_pool_reuses_blocks_and_trims(cuda_device):
+    """gb_graph_free caches the graph's device blocks for the next upload of
+    the same shape; results stay right across reuse, and gb_pool_trim frees
+    the cache."""
+    from galois_b200 import _lib, rmat
+
+    g, perm = rmat(12, 8, seed=91)
+    want = oracle.bfs_serial(g, int(perm[0]))
+    first = None
+    for _ in range(3):
+        with DeviceGraph(g, symmetric=True) as dg:
+            ptrs = dg.device_arrays()
+            if first is None:
+                first = ptrs["col"]
+            else:
+                assert ptrs["col"] == first  # served from the cache
+            assert (dg.bfs(int(perm[0])) == want).all()
+    _lib.check(_lib.lib.gb_pool_trim(), "gb_pool_trim")
+    with DeviceGraph(g, symmetric=True) as dg:  # a fresh allocation after the trim
+        assert (dg.bfs(int(perm[0])) == want).all()
