@@ -335,8 +335,10 @@ class CcJob(Job):
         return float(self.graphs[gi]["host"].m)
 
     def algo_bytes(self, st, gi):
+        # column + label per arc actually scanned (a later round scans only the
+        # rows outside the giant component), offsets + label per vertex per round
         g = self.graphs[gi]["host"]
-        return st["rounds"] * (8.0 * g.m + 16.0 * g.n)
+        return 8.0 * st["edges_scanned"] + 16.0 * g.n * st["rounds"]
 
     def cpu_call(self, gi):
         import oracle

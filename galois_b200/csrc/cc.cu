@@ -13,14 +13,17 @@
 //                    smaller with atomicMin, then every vertex jumps to its
 //                    root.  p[x] <= x always holds and sum(p) strictly drops
 //                    while anything changes, so it terminates with p = min id.
+//                    On a symmetric graph rounds after the first scan only
+//                    the vertices outside the sampled giant component.
 //   GB_CC_UNIONFIND  one sweep of lock-free union-find (larger root linked
 //                    under the smaller with atomicCAS, path halving), then a
 //                    compression sweep.  Same labels.
 //   GB_CC_AFFOREST   neighbour sampling (first 2 arcs of every vertex), a
 //                    compression, detection of the most frequent root, then
 //                    union-find only over vertices outside that component.
-// On a symmetric graph each undirected edge is processed once (u > v); on a
-// directed graph every arc is processed, giving weakly connected components.
+// On a symmetric graph each undirected edge is processed once (u > v) in a
+// full sweep; on a directed graph every arc is processed, giving weakly
+// connected components.
 
 #include "device_common.cuh"
 #include "device_graph.cuh"
@@ -93,6 +96,35 @@ __device__ __forceinline__ void compress_all(CcArgs& a, uint64_t gtid, uint64_t 
   }
 }
 
+// Most frequent label among 1024 evenly spaced vertices (Afforest's estimate
+// of the giant component), written to ctl->giant.  Called by every thread of
+// one CTA.
+template <int BLOCK>
+__device__ void sample_giant(const CcArgs& a, CcCtl* ctl) {
+  __shared__ uint32_t s_root[1024];
+  __shared__ uint32_t s_cnt[1024];
+  for (uint32_t i = threadIdx.x; i < 1024; i += BLOCK) {
+    const uint32_t v = (uint32_t)(((uint64_t)i * a.n) >> 10);
+    s_root[i] = a.p[v];
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < 1024; i += BLOCK) {
+    uint32_t c = 0;
+    for (uint32_t j = 0; j < 1024; ++j) c += s_root[j] == s_root[i];
+    s_cnt[i] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t best = s_root[0], bestc = 0;
+    for (uint32_t i = 0; i < 1024; ++i)
+      if (s_cnt[i] > bestc) {
+        bestc = s_cnt[i];
+        best = s_root[i];
+      }
+    ctl->giant = best;
+  }
+}
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
   CcCtl* ctl = a.ctl;
@@ -102,11 +134,21 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
   const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
   const uint32_t lane = lane_id();
   unsigned long long my_scanned = 0;
+  // After the first round (and its compression) every label is a root.  On a
+  // symmetric graph a later round then scans only the rows of vertices whose
+  // label is not the sampled giant label, each in full (both arc directions):
+  // an arc whose ends disagree has at least one end outside the giant
+  // component, and that end's row holds it (the skip Afforest makes,
+  // applied to label propagation).  Most vertices join the giant component
+  // in the first round, so the confirming round reads few arcs.
+  uint32_t giant = 0xFFFFFFFFu;
   for (uint32_t r = 0;; ++r) {
     if (r >= a.max_rounds) {
       if (gtid == 0) raise_err(&ctl->err, kDevMaxRounds);
       break;
     }
+    const bool skip_giant = a.half && r >= 1;
+    const bool all_dirs = !a.half || skip_giant;  // arcs u < v too
     uint32_t* changed = &ctl->changed[r % 3];
     if (gtid == 0) ctl->changed[(r + 1) % 3] = 0;
     bool my_change = false;
@@ -129,8 +171,9 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
     const uint64_t total = nchunks + a.sched.ntiles;
     // one tile of a heavy row: 8 column loads, then 8 label loads, per lane
     auto tile_fn = [&](uint32_t v, uint64_t b, uint64_t e) {
-      if (lane == 0) my_scanned += e - b;
       const uint32_t pv = a.p[v];
+      if (skip_giant && pv == giant) return;  // warp-uniform
+      if (lane == 0) my_scanned += e - b;
       constexpr int UT = 8;
       for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
         uint32_t u[UT], pu[UT];
@@ -138,7 +181,7 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
         for (int k = 0; k < UT; ++k) {
           const uint64_t i = i0 + lane + 32 * k;
           const uint32_t x = i < e ? ldg(a.col + i) : 0u;
-          u[k] = (i < e && (!a.half || x > v)) ? x : 0xFFFFFFFFu;
+          u[k] = (i < e && (all_dirs || x > v)) ? x : 0xFFFFFFFFu;
         }
 #pragma unroll
         for (int k = 0; k < UT; ++k) pu[k] = u[k] != 0xFFFFFFFFu ? a.p[u[k]] : 0u;
@@ -156,13 +199,14 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
           const uint64_t dd = ldg(a.offs + v64 + 1) - b;
           d = dd > a.sched.heavy ? 0u : (uint32_t)dd;
           pv = a.p[v64];
+          if (skip_giant && pv == giant) d = 0;
         }
         my_scanned += d;
         warp_expand_mlp<4, uint32_t>(
             b, d, (uint32_t)v64,
             [&](bool valid, uint64_t e, uint32_t v) {
               const uint32_t u = valid ? ldg(a.col + e) : 0u;
-              return (valid && (!a.half || u > v)) ? u : 0xFFFFFFFFu;
+              return (valid && (all_dirs || u > v)) ? u : 0xFFFFFFFFu;
             },
             [&](bool, uint64_t, uint32_t u, uint32_t) { return u != 0xFFFFFFFFu ? a.p[u] : 0u; },
             [&](bool, uint32_t owner, uint32_t, uint32_t u, uint32_t pu) {
@@ -184,6 +228,11 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     if (gtid == 0) ctl->rounds = r + 1;
     if (*reinterpret_cast<volatile uint32_t*>(changed) == 0) break;
+    if (r == 0 && a.half) {
+      if (blockIdx.x == 0) sample_giant<BLOCK>(a, ctl);
+      if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+      giant = *reinterpret_cast<volatile uint32_t*>(&ctl->giant);
+    }
   }
   my_scanned = warp_sum(my_scanned);
   if (lane == 0 && my_scanned) atomicAdd(&ctl->scanned, my_scanned);
@@ -210,27 +259,7 @@ __global__ void __launch_bounds__(BLOCK) cc_unionfind(CcArgs a, int afforest) {
     compress_all(a, gtid, gthreads);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     // 2. most frequent root among 1024 evenly spaced vertices
-    if (blockIdx.x == 0) {
-      __shared__ uint32_t s_root[1024];
-      __shared__ uint32_t s_cnt[1024];
-      for (uint32_t i = threadIdx.x; i < 1024; i += BLOCK) {
-        const uint32_t v = (uint32_t)(((uint64_t)i * a.n) >> 10);
-        s_root[i] = a.p[v];
-      }
-      __syncthreads();
-      for (uint32_t i = threadIdx.x; i < 1024; i += BLOCK) {
-        uint32_t c = 0;
-        for (uint32_t j = 0; j < 1024; ++j) c += s_root[j] == s_root[i];
-        s_cnt[i] = c;
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        uint32_t best = s_root[0], bestc = 0;
-        for (uint32_t i = 0; i < 1024; ++i)
-          if (s_cnt[i] > bestc) { bestc = s_cnt[i]; best = s_root[i]; }
-        ctl->giant = best;
-      }
-    }
+    if (blockIdx.x == 0) sample_giant<BLOCK>(a, ctl);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     giant = *reinterpret_cast<volatile uint32_t*>(&ctl->giant);
   }
