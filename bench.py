@@ -233,6 +233,12 @@ class Job:
     def algo_bytes(self, st: dict, gi: int) -> float:
         raise NotImplementedError
 
+    def work_bytes(self, st: dict, gi: int) -> float:
+        """Bytes of the arcs the kernel actually scanned (the algorithmic model
+        counts every reached arc once; direction-optimised BFS and the giant
+        skip of CC read fewer, label-correcting SSSP reads more)."""
+        return self.algo_bytes(st, gi)
+
     def cpu_call(self, gi):
         raise NotImplementedError
 
@@ -276,6 +282,9 @@ class SsspJob(Job):
         # col + weight + dist per arc; offsets (16), dist write, queue push/pop per vertex
         return 12.0 * st["edges_reached"] + 28.0 * st["vertices_reached"]
 
+    def work_bytes(self, st, gi):
+        return 12.0 * st["edges_scanned"] + 28.0 * st["vertices_reached"]
+
     def cpu_call(self, gi):
         import oracle
 
@@ -306,6 +315,9 @@ class BfsJob(Job):
     def algo_bytes(self, st, gi):
         return 8.0 * st["edges_reached"] + 28.0 * st["vertices_reached"]
 
+    def work_bytes(self, st, gi):
+        return 8.0 * st["edges_scanned"] + 28.0 * st["vertices_reached"]
+
     def cpu_call(self, gi):
         import oracle
 
@@ -335,8 +347,12 @@ class CcJob(Job):
         return float(self.graphs[gi]["host"].m)
 
     def algo_bytes(self, st, gi):
-        # column + label per arc actually scanned (a later round scans only the
-        # rows outside the giant component), offsets + label per vertex per round
+        # one sweep = column + label per arc, offsets + label per vertex; counted per round
+        g = self.graphs[gi]["host"]
+        return st["rounds"] * (8.0 * g.m + 16.0 * g.n)
+
+    def work_bytes(self, st, gi):
+        # a round after the first scans only the rows outside the giant component
         g = self.graphs[gi]["host"]
         return 8.0 * st["edges_scanned"] + 16.0 * g.n * st["rounds"]
 
@@ -723,6 +739,7 @@ def main() -> None:
     stats = st_runs[-1]
     units_step = sum(job.units(st, gi) for gi, st in enumerate(stats))
     bytes_step = sum(job.algo_bytes(st, gi) for gi, st in enumerate(stats))
+    work_step = sum(job.work_bytes(st, gi) for gi, st in enumerate(stats))
     # the first call of a kernel also pays its lazy module load: average the later runs
     kms = [sum(r[gi]["kernel_ms"] for r in st_runs[1:]) / (len(st_runs) - 1) for gi in range(len(dgs))]
     for _ in range(args.warmup):
@@ -751,6 +768,9 @@ def main() -> None:
                 # a degree-ordered PageRank runs the flat pull kernel
                 "kernel": "pr_pull_flat" if (isinstance(job, PrJob) and args.order) else job.kernel,
                 "algorithmic_bytes_per_step": bytes_step, "kernel_ms_per_step": sum(kms),
+                # the same over the arcs the kernel actually read
+                "work_bytes_per_step": work_step,
+                "frac_of_work": work_step / (sum(kms) / 1e3) / 1e9 / peak,
                 "traffic": traffic_from_profiles(f"{args.app}-{args.size}")}
     line = {"metric": job.metric, "value": value, "unit": job.unit, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
