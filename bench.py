@@ -121,49 +121,96 @@ def aggregate_rate(world: int, units_per_step: float, steps: int, t_ms_max: floa
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) of the SM clock and throttle reasons."""
+    """SM clock and throttle reasons during a timed region: nvidia-smi at its
+    200 ms period plus an NVML thread at 1 ms, so that timed regions shorter
+    than nvidia-smi's period still get samples.  The GPU is named by its UUID
+    (CUDA and NVML number devices differently under CUDA_VISIBLE_DEVICES)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu: int):
+    def __init__(self, gpu: int, period_s: float = 0.001):
         self.gpu = gpu
+        self.period_s = period_s
         self.proc = None
+        self.thread = None
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.uuid = None
+        try:
+            import torch
+
+            self.uuid = "GPU-" + str(torch.cuda.get_device_properties(gpu).uuid)
+        except Exception:
+            pass
+
+    def _nvml_loop(self, stop, rows):
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+        except Exception:
+            return
+        try:
+            h = nv.nvmlDeviceGetHandleByUUID(self.uuid) if self.uuid else nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            while not stop.is_set():
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                rows.append((sm, smax, tuple(bool(mask & b) for b in bits)))
+                stop.wait(self.period_s)
+        except Exception:
+            pass
+        finally:
+            try:
+                nv.nvmlShutdown()
+            except Exception:
+                pass
 
     def start(self):
+        import threading
+
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.uuid or str(self.gpu), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.file, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        self._stop = threading.Event()
+        self._nvml_rows = []
+        self.thread = threading.Thread(target=self._nvml_loop, args=(self._stop, self._nvml_rows), daemon=True)
+        self.thread.start()
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.file.flush()
-        rows = []
-        for line in Path(self.file.name).read_text().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join(timeout=5)
+        rows = []  # (sm MHz, max MHz, (reason active,) * 4)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.file.flush()
+            for line in Path(self.file.name).read_text().splitlines():
+                r = [x.strip() for x in line.split(",")]
+                if len(r) >= 9 and r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+                    rows.append((float(r[1]), float(r[2]), tuple(r[5 + i].lower() == "active" for i in range(4))))
         os.unlink(self.file.name)
+        n_smi = len(rows)
+        rows += self._nvml_rows if self.thread is not None else []
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        loaded = [s for s in sm if s > 0.5 * smax] or sm
-        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
-                "reasons": reasons, "samples": len(rows)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [] if self.proc else ["nvidia-smi unavailable"],
+                    "samples": 0}
+        smax = max(r[1] for r in rows)
+        reasons = sorted({self.REASONS[i] for r in rows for i in range(4) if r[2][i]})
+        loaded = [r[0] for r in rows if r[0] > 0.5 * smax] or [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows), "samples_nvidia_smi": n_smi, "samples_nvml": len(rows) - n_smi}
 
 
 def measured_peak_hbm() -> tuple[float, str]:

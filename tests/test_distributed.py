@@ -158,3 +158,18 @@ def test_aggregate_rate_is_whole_job(world):
     bench = _bench()
     # 1e9 units per rank per step, 4 steps, slowest rank 2 s -> world*2 G/s
     assert bench.aggregate_rate(world, 1e9, 4, 2000.0) == pytest.approx(2.0 * world)
+
+
+def test_clock_sampler_merges_fast_samples():
+    """Timed regions shorter than nvidia-smi's 200 ms period still get clock
+    samples from the 1 ms NVML thread; idle-clock samples are left out of the
+    median and any throttle reason seen is reported."""
+    c = _bench().ClockSampler(0)
+    c.start()
+    c._nvml_rows += [(1965.0, 1965.0, (False, False, False, True)),
+                     (1900.0, 1965.0, (False,) * 4), (210.0, 1965.0, (False,) * 4)]
+    got = c.stop()
+    assert got["sm_mhz"] == pytest.approx(1932.5)
+    assert got["sm_max_mhz"] == 1965.0
+    assert got["reasons"] == ["sw_power_cap"]
+    assert got["samples_nvml"] >= 3
