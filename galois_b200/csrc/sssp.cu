@@ -21,7 +21,19 @@
 //     costs two dependent memory round trips (arcs, then the atomic with the
 //     target's offsets);
 //   * a far pile holding vertices relaxed beyond the bucket (membership
-//     bitmap, so each vertex is in the pile at most once).
+//     bitmap, so each vertex is in the pile at most once);
+//   * for large frontiers, a bitmap instead of the near queue: a phase whose
+//     input frontier is estimated above `bm_min` relaxes with reductions
+//     that return nothing (red.min on the distance, red.or on the next
+//     phase's bitmap), so a warp step never waits on an atomic's reply, and
+//     the next phase sweeps the bitmap in id order (light rows 1024 ids per
+//     warp step, heavy rows from the graph's cached tile schedule).  Three
+//     bitmaps rotate: phase P reads P%3, sets (P+1)%3 and clears (P+2)%3, so
+//     no word is cleared by plain stores in the phase right after atomics
+//     updated it.  Queue entries and bitmap bits are two encodings of the
+//     same set (vertices whose distance dropped inside the bucket); the
+//     distance is read when the vertex is expanded, so either encoding gives
+//     the same fixed point.
 // Work is spread over warps statically (no work-grabbing atomics).  When the
 // near queue drains, the far pile is split: settled entries are dropped, the
 // minimum remaining bucket becomes current (empty buckets are skipped), its
@@ -31,6 +43,7 @@
 #include "device_common.cuh"
 #include "device_graph.cuh"
 #include "frontier.cuh"
+#include "sweep.cuh"
 
 namespace gb {
 
@@ -39,6 +52,14 @@ namespace {
 constexpr int kLocalQ = 64;  // local-queue entries per warp
 constexpr int kStage = 64;   // near-queue appends staged per warp before publishing
 constexpr uint32_t kNotQueued = 0xFFFFFFFFu;
+
+// Reductions whose result is not needed: the SM issues them and moves on.
+__device__ __forceinline__ void red_min_u32(uint32_t* p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.min.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_or_u32(uint32_t* p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 struct SsspCtl {
   GridBar bar;
@@ -72,6 +93,10 @@ struct SsspArgs {
   uint32_t max_phases;
   int local_depth;
   int all_light;  // max degree <= heavy: skip the degree lookup when queueing
+  uint32_t* act[3];      // frontier bitmaps (phase P reads act[P % 3])
+  const uint2* sw_tiles;  // cached (vertex, k) tiles of every heavy vertex
+  uint32_t sw_ntiles;
+  uint32_t bm_min;  // frontier estimate above which the next frontier is a bitmap
 };
 
 __global__ void sssp_init(SsspArgs a) {
@@ -82,7 +107,12 @@ __global__ void sssp_init(SsspArgs a) {
     a.dist[v] = (v == a.src) ? 0u : kInf;
     a.stamp[v] = (v == a.src) ? 0u : kNotQueued;
   }
-  for (uint64_t w = tid; w < words; w += stride) a.infar[w] = 0;
+  for (uint64_t w = tid; w < words; w += stride) {
+    a.infar[w] = 0;
+    a.act[0][w] = 0;
+    a.act[1][w] = 0;
+    a.act[2][w] = 0;
+  }
   if (tid == 0) {
     const uint64_t d = a.offs[a.src + 1] - a.offs[a.src];
     FrontierCounters& c = a.ctl->fc[0];
@@ -92,7 +122,10 @@ __global__ void sssp_init(SsspArgs a) {
   }
 }
 
-template <int BLOCK>
+// kBitmap: large frontiers may switch to the bitmap encoding (power-law
+// graphs); off, the kernel is the queue-only form that low-degree,
+// high-diameter graphs (small frontiers, local queues) run.
+template <int BLOCK, bool kBitmap>
 __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
   __shared__ uint4 s_lq[BLOCK / 32][kLocalQ];
   __shared__ uint32_t s_stage[BLOCK / 32][kStage];
@@ -104,12 +137,17 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
   const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
   const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
   const unsigned lanemask_lt = (1u << lane) - 1u;
+  __shared__ uint32_t s_push;
   uint4* lq = s_lq[threadIdx.x >> 5];
   unsigned long long my_scanned = 0, my_relax = 0;
+  const uint32_t words = (a.n + 31) >> 5;
+  if (threadIdx.x == 0) s_push = 0;
 
   uint32_t bucket = 0;  // current bucket index; near items have dist < hi
   int fp = 0;           // far pile being appended to
   uint32_t P = 0;       // phase counter (counter set P%3, queue buffer P&1)
+  bool bm_in = false;   // this phase's frontier is the bitmap act[P % 3]
+  uint32_t dirty = 0;   // bit i: act[i] may hold set bits
 
   for (;;) {
     if (P >= a.max_phases) {
@@ -129,9 +167,27 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
     const uint32_t hi = hi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)hi64;
     uint32_t* farq = a.far[fp];
     const int qnext = (P + 1) & 1;
+    // the bitmap that phase P+1 sets was read in phase P-1 and last set in
+    // phase P-2: cleared now, with no atomics on it in flight
+    {
+      const int clr = (int)((P + 2) % 3);
+      if (dirty & (1u << clr)) {
+        uint32_t* c = a.act[clr];
+        for (uint64_t i = gtid; i < words; i += gthreads) c[i] = 0;
+        dirty &= ~(1u << clr);
+      }
+    }
+    // bitmap input: the count of bit-setting reductions of the last phase
+    // (an upper bound on the vertices set; zero means an empty frontier)
+    const uint32_t bm_count = bm_in ? cur.vertices : 0u;
 
-    if (q_light != 0 || q_tiles != 0) {
+    if (kBitmap && bm_in ? bm_count != 0 : (q_light != 0 || q_tiles != 0)) {
       // ---- relaxation phase --------------------------------------------
+      // every thread reads the same counters, so the choice is grid-uniform
+      const uint64_t est = bm_in ? (uint64_t)bm_count : (uint64_t)q_light + 8ull * q_tiles;
+      const bool bm_out = kBitmap && est > a.bm_min;
+      uint32_t* const act_next = a.act[(P + 1) % 3];
+      uint32_t my_push = 0;  // lane 0: this warp's bit-setting reductions
       uint32_t lq_n = 0;  // warp-uniform local queue length
       WarpStage<kStage> stage{s_stage[threadIdx.x >> 5], 0u};
       uint32_t* const nq = a.fq.light[qnext];
@@ -172,6 +228,29 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
       // stale value only costs an extra atomic; the atomicMin decides)
       auto relax = [&](bool valid, uint32_t u, uint32_t nd, uint32_t du) {
         bool near = false, far = false;
+        if (bm_out) {
+          // no reply awaited: the bit marks u for the next phase, which reads
+          // dist[u] when it expands u (a bit set by a candidate that lost to
+          // a smaller one only costs that re-expansion)
+          if (valid && nd < du) {
+            red_min_u32(&a.dist[u], nd);
+            const uint32_t bit = 1u << (u & 31);
+            if (nd < hi) {
+              red_or_u32(&act_next[u >> 5], bit);
+              near = true;
+            } else if (!(a.infar[u >> 5] & bit)) {
+              far = !(atomicOr(&a.infar[u >> 5], bit) & bit);
+            }
+          }
+          const unsigned nm = __ballot_sync(kFull, near);
+          const unsigned rm = __ballot_sync(kFull, near || far);
+          if (lane == 0) {
+            my_push += __popc(nm);
+            my_relax += __popc(rm);
+          }
+          if (__any_sync(kFull, far)) warp_push(far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
+          return;
+        }
         uint64_t ub = 0, deg = 1;
         if (valid && nd < du) {
           // the offset loads do not depend on the atomic: issued together
@@ -214,56 +293,106 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
       };
       const uint32_t* qin = a.fq.light[P & 1];
       const uint2* tin = a.fq.tiles[P & 1];
-      // A large frontier is swept densely: every vertex in id order, active
-      // when its stamp names this phase (it was queued for it and not queued
-      // again since; a vertex re-queued for the next phase is expanded there
-      // with its newer distance).  Consecutive rows keep the column and
-      // weight reads contiguous, which the queue's arbitrary order does not.
-      const bool dense = q_light > (a.n >> 4);
-      const uint32_t nl = dense ? a.n : q_light;
-      for_each_frontier_task(
-          nl, q_tiles, gwarp, nwarps,
-          [&](uint32_t base, uint32_t vpt) {
-            const uint32_t idx = base + lane;
-            const bool has = lane < vpt && idx < nl;
+      // one heavy tile: arcs [k*tile, (k+1)*tile) of v, by the whole warp
+      auto tile_body = [&](uint32_t v, uint32_t k) {
+        const uint64_t vb = ldg(a.offs + v), ve = ldg(a.offs + v + 1);
+        const uint64_t b = vb + (uint64_t)k * a.tile;
+        const uint64_t e_end = min(ve, b + a.tile);
+        const uint32_t dsrc = __ldcg(a.dist + v);
+        if (lane == 0) my_scanned += e_end - b;
+        constexpr int U = 4;
+        for (uint64_t e0 = b; e0 < e_end; e0 += 32 * U) {
+          uint32_t u[U], nd[U], du[U];
+          bool valid[U];
+#pragma unroll
+          for (int k = 0; k < U; ++k) {
+            const uint64_t e = e0 + 32 * k + lane;
+            valid[k] = e < e_end;
+            u[k] = valid[k] ? ldg(a.col + e) : 0u;
+          }
+#pragma unroll
+          for (int k = 0; k < U; ++k) {
+            const uint64_t e = e0 + 32 * k + lane;
+            nd[k] = valid[k] ? dsrc + ldg(a.w + e) : 0u;
+            du[k] = valid[k] ? a.dist[u[k]] : 0u;
+          }
+#pragma unroll
+          for (int k = 0; k < U; ++k) relax(valid[k], u[k], nd[k], du[k]);
+        }
+      };
+      if (kBitmap && bm_in) {
+        // bitmap frontier: a warp owns words gwarp, gwarp + nwarps, ... (32
+        // ids each; strided so that the dense low ids of a degree-ordered
+        // graph spread over all warps), loads 32 of them per step and expands
+        // the non-zero ones one at a time, one vertex per lane
+        const uint32_t* act = a.act[P % 3];
+        for (uint64_t base = gwarp; base < words; base += nwarps << 5) {
+          const uint64_t wi = base + (uint64_t)lane * nwarps;
+          const uint32_t word = wi < words ? __ldcg(act + wi) : 0u;
+          unsigned nz = __ballot_sync(kFull, word != 0u);
+          while (nz) {
+            const int j = __ffs(nz) - 1;
+            nz &= nz - 1u;
+            const uint32_t bits = __shfl_sync(kFull, word, j);
+            const uint32_t v = (uint32_t)((base + (uint64_t)j * nwarps) << 5) + lane;  // < n when its bit is set
             uint64_t b = 0;
             uint32_t d = 0, dv = 0;
-            if (has) {
-              const uint32_t v = dense ? idx : qin[idx];
+            if ((bits >> lane) & 1u) {
               b = ldg(a.offs + v);
-              d = (uint32_t)(ldg(a.offs + v + 1) - b);
-              dv = __ldcg(a.dist + v);
-              if (dense && (a.stamp[v] != P || d > a.heavy)) d = 0;  // not this phase's light vertex
+              const uint64_t dd = ldg(a.offs + v + 1) - b;
+              if (dd <= a.heavy) {
+                d = (uint32_t)dd;
+                dv = __ldcg(a.dist + v);
+              }
             }
             expand(b, d, dv, dv, true);
-          },
-          [&](uint32_t t) {
-            const uint2 tv = tin[t];
-            const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
-            const uint64_t b = vb + (uint64_t)tv.y * a.tile;
-            const uint64_t e_end = min(ve, b + a.tile);
-            const uint32_t dsrc = __ldcg(a.dist + tv.x);
-            if (lane == 0) my_scanned += e_end - b;
-            constexpr int U = 4;
-            for (uint64_t e0 = b; e0 < e_end; e0 += 32 * U) {
-              uint32_t u[U], nd[U], du[U];
-              bool valid[U];
-#pragma unroll
-              for (int k = 0; k < U; ++k) {
-                const uint64_t e = e0 + 32 * k + lane;
-                valid[k] = e < e_end;
-                u[k] = valid[k] ? ldg(a.col + e) : 0u;
+          }
+        }
+        // heavy vertices: the cached tile schedule, strided the same way
+        for (uint64_t t0 = gwarp; t0 < a.sw_ntiles; t0 += nwarps << 5) {
+          const uint64_t ti = t0 + (uint64_t)lane * nwarps;
+          uint2 tv = make_uint2(0u, 0u);
+          bool on = false;
+          if (ti < a.sw_ntiles) {
+            tv = a.sw_tiles[ti];
+            on = (__ldcg(act + (tv.x >> 5)) >> (tv.x & 31)) & 1u;
+          }
+          unsigned m = __ballot_sync(kFull, on);
+          while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1u;
+            tile_body(__shfl_sync(kFull, tv.x, j), __shfl_sync(kFull, tv.y, j));
+          }
+        }
+      } else {
+        // A large queue is swept densely: every vertex in id order, active
+        // when its stamp names this phase (it was queued for it and not
+        // queued again since; a vertex re-queued for the next phase is
+        // expanded there with its newer distance).  Consecutive rows keep the
+        // column and weight reads contiguous, which the queue's order does not.
+        const bool dense = q_light > (a.n >> 4);
+        const uint32_t nl = dense ? a.n : q_light;
+        for_each_frontier_task(
+            nl, q_tiles, gwarp, nwarps,
+            [&](uint32_t base, uint32_t vpt) {
+              const uint32_t idx = base + lane;
+              const bool has = lane < vpt && idx < nl;
+              uint64_t b = 0;
+              uint32_t d = 0, dv = 0;
+              if (has) {
+                const uint32_t v = dense ? idx : qin[idx];
+                b = ldg(a.offs + v);
+                d = (uint32_t)(ldg(a.offs + v + 1) - b);
+                dv = __ldcg(a.dist + v);
+                if (dense && (a.stamp[v] != P || d > a.heavy)) d = 0;  // not this phase's light vertex
               }
-#pragma unroll
-              for (int k = 0; k < U; ++k) {
-                const uint64_t e = e0 + 32 * k + lane;
-                nd[k] = valid[k] ? dsrc + ldg(a.w + e) : 0u;
-                du[k] = valid[k] ? a.dist[u[k]] : 0u;
-              }
-#pragma unroll
-              for (int k = 0; k < U; ++k) relax(valid[k], u[k], nd[k], du[k]);
-            }
-          });
+              expand(b, d, dv, dv, true);
+            },
+            [&](uint32_t t) {
+              const uint2 tv = tin[t];
+              tile_body(tv.x, tv.y);
+            });
+      }
       // local rounds: keep relaxing what this warp lowered (LIFO), with no
       // distance pre-check (low-degree targets: the atomic is cheaper than
       // another dependent load)
@@ -290,6 +419,16 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
         stage.push(to_near, ent.x, nq, &nxt.light, a.fq.light_cap, &ctl->err);  // local entries are light
       }
       stage.flush(nq, &nxt.light, a.fq.light_cap, &ctl->err);
+      if (bm_out) {  // grid-uniform branch: the CTA's bit-setting reductions, added once
+        if (lane == 0 && my_push) atomicAdd_block(&s_push, my_push);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          if (s_push) atomicAdd(&nxt.vertices, s_push);
+          s_push = 0;
+        }
+        dirty |= 1u << ((P + 1) % 3);
+      }
+      bm_in = bm_out;
       if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
       ++P;
       continue;
@@ -342,6 +481,7 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
     }
     bucket = nb;
     fp ^= 1;
+    bm_in = false;  // the split filled the near queue
     if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
     ++P;
   }
@@ -384,7 +524,12 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   const uint32_t words = (n + 31) / 32;
   const bool out_dev = is_device_ptr(dist_out);
   FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
-  const size_t need = carve_size<SsspCtl>(1) + carve_size<uint32_t>(n) + carve_size<uint32_t>(words) +
+  SweepSched sched{};
+  if (g->max_degree > t.heavy_degree) {  // heavy rows of a bitmap frontier come from the tile schedule
+    int sst = ensure_sweep_schedule(g, t.heavy_degree, t.tile_edges, s, &sched);
+    if (sst != GB_OK) return sst;
+  }
+  const size_t need = carve_size<SsspCtl>(1) + carve_size<uint32_t>(n) + 4 * carve_size<uint32_t>(words) +
                       2 * carve_size<uint32_t>(n) + fl.bytes + (out_dev ? 0 : carve_size<uint32_t>(n)) +
                       carve_size<unsigned long long>(2);
   int st = ws_reserve(g, need, s);
@@ -394,6 +539,7 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   a.ctl = cv.take<SsspCtl>(1);
   a.stamp = cv.take<uint32_t>(n);
   a.infar = cv.take<uint32_t>(words);
+  for (int i = 0; i < 3; ++i) a.act[i] = cv.take<uint32_t>(words);
   a.far[0] = cv.take<uint32_t>(n);
   a.far[1] = cv.take<uint32_t>(n);
   a.fq = carve_frontier(cv, fl);
@@ -410,13 +556,24 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   a.max_phases = 0x7FFFFFFFu;
   a.local_depth = t.local_depth < 0 ? 0 : t.local_depth;
   a.all_light = g->max_degree <= t.heavy_degree ? 1 : 0;
+  a.sw_tiles = sched.tiles;
+  a.sw_ntiles = sched.ntiles;
+  // a frontier of more than n/64 vertices (a tile counting as 8) makes the
+  // next one a bitmap: its sweep reads n/8 bytes of bitmap, small beside the
+  // arcs of such a frontier
+  a.bm_min = n >> 6;
   GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), s));
   sssp_init<<<g->sm_count * 4, 256, 0, s>>>(a);
   GB_CUDA(cudaGetLastError());
   const bool big = t.block_threads >= 1024;
   const int block = big ? 1024 : 256;
-  const void* kfn = big ? reinterpret_cast<const void*>(&sssp_persistent<1024>)
-                        : reinterpret_cast<const void*>(&sssp_persistent<256>);
+  // local queues serve small frontiers; only without them can a frontier
+  // grow large enough for the bitmap
+  const bool bm = a.local_depth == 0;
+  const void* kfn = big ? (bm ? reinterpret_cast<const void*>(&sssp_persistent<1024, true>)
+                              : reinterpret_cast<const void*>(&sssp_persistent<1024, false>))
+                        : (bm ? reinterpret_cast<const void*>(&sssp_persistent<256, true>)
+                              : reinterpret_cast<const void*>(&sssp_persistent<256, false>));
   const int grid = coop_grid(g, kfn, block, 0, t.blocks_per_sm);
   if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
   void* args[] = {&a};
