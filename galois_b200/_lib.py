@@ -118,6 +118,7 @@ SIGNATURES: dict[str, tuple] = {
     "gb_graph_set_tuning": (C.c_int, [_gp, C.POINTER(Tuning)]),
     "gb_graph_get_tuning": (C.c_int, [_gp, C.POINTER(Tuning)]),
     "gb_bfs": (C.c_int, [_gp, C.c_uint32, _vp, C.POINTER(Stats), _vp]),
+    "gb_bfs_parent": (C.c_int, [_gp, C.c_uint32, _vp, _vp, C.POINTER(Stats), _vp]),
     "gb_bfs_noalloc": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint64, C.c_int, C.c_uint32, _vp, _vp]),
     "gb_sssp_delta": (C.c_int, [_gp, C.c_uint32, C.c_uint32, _vp, C.POINTER(Stats), _vp]),
     "gb_cc": (C.c_int, [_gp, C.c_int, _vp, C.POINTER(Stats), _vp]),

@@ -159,6 +159,17 @@ class DeviceGraph:
         check(lib.gb_bfs(self.handle, src, ptr, C.byref(s) if s else None, stream), "gb_bfs")
         return (obj, s.as_dict()) if stats else obj
 
+    def bfs_parent(self, src: int, out=None, level_out=None, stats: bool = False):
+        """Parents of a BFS tree from src (bfsDirectionOpt's output): the
+        smallest-id in-neighbour one level closer; 0 at src, INF unreached."""
+        ptr, stream, obj = self._out(out, self.n, np.uint32, "parent_out")
+        lptr = None
+        if level_out is not None:
+            lptr, _, _ = self._out(level_out, self.n, np.uint32, "level_out")
+        s = self._stats(stats)
+        check(lib.gb_bfs_parent(self.handle, src, ptr, lptr, C.byref(s) if s else None, stream), "gb_bfs_parent")
+        return (obj, s.as_dict()) if stats else obj
+
     def sssp(self, src: int, delta_shift: int = 13, out=None, stats: bool = False):
         ptr, stream, obj = self._out(out, self.n, np.uint32, "dist_out")
         s = self._stats(stats)

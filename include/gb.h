@@ -209,6 +209,18 @@ int gb_graph_get_tuning(const gb_graph* g, gb_tuning* t);
 int gb_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats,
            void* stream);
 
+/* BFS parents from src, the output of the direction-optimising lonestar BFS
+ * (bfsDirectionOpt.cpp:204-342, which stores the parent, not the level:
+ * :284-285, :325).  parent_out[src] = 0 as the reference leaves the source's
+ * datum (:229); unreached = GB_DIST_INFINITY; every other reached v gets the
+ * smallest id among its in-neighbours one level closer to src -- the
+ * reference keeps whichever such in-neighbour wins a compare-and-swap, so
+ * this is one of its possible outputs, made reproducible.  level_out
+ * (nullable) receives the levels as gb_bfs gives them.  A directed graph
+ * needs its in-edges: the transpose is built on first use. */
+int gb_bfs_parent(gb_graph* g, uint32_t src, uint32_t* parent_out,
+                  uint32_t* level_out, gb_stats* stats, void* stream);
+
 /* Allocation-free BFS (no counterpart in the reference).  For callers that
  * cannot call cudaMalloc -- e.g. a host application that owns and budgets all
  * device memory and forbids libraries from allocating -- this runs the gb_bfs

@@ -48,6 +48,9 @@ _SIG = {
     "orc_bfs_serial": (None, [_u32, _vp, _vp, _u32, _vp]),
     "orc_bfs_sync_tile": (None, [_u32, _vp, _vp, _u32, _vp]),
     "orc_verify_bfs": (C.c_int, [_u32, _vp, _vp, _u32, _vp]),
+    "orc_bfs_do_parent": (None, [_u32, _vp, _vp, _vp, _vp, _u32, C.c_int, C.c_int, _vp]),
+    "orc_bfs_parent_min": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
+    "orc_verify_bfs_parent": (C.c_int, [_u32, _vp, _vp, _vp, _u32, _vp]),
     "orc_sssp_dijkstra": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
     "orc_sssp_delta_serial": (None, [_u32, _vp, _vp, _vp, _u32, _u32, _vp]),
     "orc_sssp_delta_parallel": (None, [_u32, _vp, _vp, _vp, _u32, _u32, _vp]),
@@ -111,6 +114,45 @@ def verify_bfs(g, src: int, level) -> int:
     n, end, col = _g(g)
     lv = np.ascontiguousarray(level, np.uint32)
     return _lib.orc_verify_bfs(n, _p(end), _p(col), src, _p(lv))
+
+
+def _in_edges(g):
+    """(in_end, in_col): the transposed graph in the same end-offset layout
+    (a symmetric graph is its own transpose)."""
+    n, end, col = _g(g)
+    deg = np.diff(np.concatenate(([0], end.astype(np.int64))))
+    rows = np.repeat(np.arange(n, dtype=np.uint32), deg)
+    order = np.lexsort((rows, col))  # by target, then source
+    in_col = np.ascontiguousarray(rows[order], dtype=np.uint32)
+    in_end = np.cumsum(np.bincount(col, minlength=n), dtype=np.uint64)
+    return in_end, in_col
+
+
+def bfs_do_parent(g, src: int, alpha: int = 15, beta: int = 18) -> np.ndarray:
+    """Serial restatement of bfsDirectionOpt's SyncDO parents."""
+    n, end, col = _g(g)
+    in_end, in_col = _in_edges(g)
+    out = np.empty(n, np.uint32)
+    _lib.orc_bfs_do_parent(n, _p(end), _p(col), _p(in_end), _p(in_col), src, alpha, beta, _p(out))
+    return out
+
+
+def bfs_parent_min(g, src: int, level) -> np.ndarray:
+    """Smallest-id in-neighbour one level closer, per reached vertex."""
+    n, _, _ = _g(g)
+    in_end, in_col = _in_edges(g)
+    lv = np.ascontiguousarray(level, np.uint32)
+    out = np.empty(n, np.uint32)
+    _lib.orc_bfs_parent_min(n, _p(in_end), _p(in_col), _p(lv), src, _p(out))
+    return out
+
+
+def verify_bfs_parent(g, src: int, level, parent) -> int:
+    n, _, _ = _g(g)
+    in_end, in_col = _in_edges(g)
+    lv = np.ascontiguousarray(level, np.uint32)
+    pa = np.ascontiguousarray(parent, np.uint32)
+    return _lib.orc_verify_bfs_parent(n, _p(in_end), _p(in_col), _p(lv), src, _p(pa))
 
 
 def sssp_dijkstra(g, src: int) -> np.ndarray:

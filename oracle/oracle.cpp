@@ -179,6 +179,120 @@ int orc_verify_bfs(uint32_t n, const uint64_t* end, const uint32_t* col, uint32_
   return 0;
 }
 
+// ---- BFS parents (bfsDirectionOpt.cpp) ---------------------------------------
+
+// Direction-optimising BFS storing parents, serial: syncDOAlgo
+// (bfsDirectionOpt.cpp:204-342) with CONCURRENT = false.  The source's datum
+// is 0 (:229, :448), unreached vertices keep DIST_INFINITY.  One work counter
+// runs through both kinds of step as in the reference: it starts at 1 (:237);
+// a push step (:303-337) resets it and adds the out-degree of every vertex
+// it reaches, giving each unvisited target the scanning vertex as parent
+// (the compare-and-swap of :325 always wins serially), and scout_count takes
+// its value; a pull step (:262-300) saves it, resets it and counts the
+// vertices it reaches, each unvisited vertex taking its first in-neighbour
+// (in in-arc order) that is in the frontier bitset (:276-290).  Pull steps
+// repeat while the count does not shrink or stays above n / beta (:299-300);
+// the switch to pull is scout_count > edges_to_check / alpha (:259).  alpha
+// and beta are ints (:68-77), so both tests divide as integers.
+void orc_bfs_do_parent(uint32_t n, const uint64_t* end, const uint32_t* col, const uint64_t* in_end,
+                       const uint32_t* in_col, uint32_t src, int alpha, int beta, uint32_t* parent) {
+  Csr g{n, end, col}, t{n, in_end, in_col};
+  for (uint32_t v = 0; v < n; ++v) parent[v] = kInf;
+  parent[src] = 0;
+  std::vector<uint32_t> curr, next{src};
+  std::vector<uint8_t> front(n, 0), nextb(n, 0);
+  uint64_t work_items = 1;
+  int64_t edges_to_check = (int64_t)(n ? end[n - 1] : 0);
+  int64_t scout = (int64_t)(g.e(src) - g.b(src));
+  while (!next.empty()) {
+    std::swap(curr, next);
+    next.clear();
+    if (scout > edges_to_check / alpha) {
+      std::fill(front.begin(), front.end(), 0);
+      for (uint32_t v : curr) front[v] = 1;
+      uint64_t old_items = 0;
+      do {
+        old_items = work_items;
+        work_items = 0;
+        for (uint32_t v = 0; v < n; ++v) {
+          if (parent[v] != kInf) continue;
+          for (uint64_t i = t.b(v); i < t.e(v); ++i) {
+            const uint32_t u = in_col[i];
+            if (front[u]) {
+              parent[v] = u;
+              nextb[v] = 1;
+              ++work_items;
+              break;
+            }
+          }
+        }
+        std::swap(front, nextb);
+        std::fill(nextb.begin(), nextb.end(), 0);
+      } while (work_items >= old_items || work_items > (uint64_t)n / (uint64_t)beta);
+      for (uint32_t v = 0; v < n; ++v)
+        if (front[v]) next.push_back(v);
+      scout = 1;
+    } else {
+      edges_to_check -= scout;
+      work_items = 0;
+      for (uint32_t v : curr) {
+        for (uint64_t i = g.b(v); i < g.e(v); ++i) {
+          const uint32_t u = col[i];
+          if (parent[u] == kInf) {
+            parent[u] = v;
+            next.push_back(u);
+            work_items += g.e(u) - g.b(u);
+          }
+        }
+      }
+      scout = (int64_t)work_items;
+    }
+  }
+}
+
+// The canonical parent tree of a BFS: every reached v other than src gets
+// the smallest id u over its in-neighbours with level[u] == level[v] - 1;
+// src gets 0, unreached vertices INF.
+void orc_bfs_parent_min(uint32_t n, const uint64_t* in_end, const uint32_t* in_col, const uint32_t* level,
+                        uint32_t src, uint32_t* parent) {
+  Csr t{n, in_end, in_col};
+  for (uint32_t v = 0; v < n; ++v) {
+    if (v == src) {
+      parent[v] = 0;
+      continue;
+    }
+    uint32_t best = kInf;
+    if (level[v] != kInf)
+      for (uint64_t i = t.b(v); i < t.e(v); ++i) {
+        const uint32_t u = in_col[i];
+        if (level[u] + 1 == level[v] && u < best) best = u;
+      }
+    parent[v] = best;
+  }
+}
+
+// A parent array is a BFS tree of src when parent[src] == 0, every other
+// vertex reached by the levels names an in-neighbour one level closer, and
+// unreached vertices hold INF.  Returns 0 when valid.
+int orc_verify_bfs_parent(uint32_t n, const uint64_t* in_end, const uint32_t* in_col, const uint32_t* level,
+                          uint32_t src, const uint32_t* parent) {
+  Csr t{n, in_end, in_col};
+  if (parent[src] != 0) return 1;
+  for (uint32_t v = 0; v < n; ++v) {
+    if (v == src) continue;
+    if (level[v] == kInf) {
+      if (parent[v] != kInf) return 2;
+      continue;
+    }
+    const uint32_t p = parent[v];
+    if (p >= n || level[p] + 1 != level[v]) return 3;
+    bool arc = false;
+    for (uint64_t i = t.b(v); i < t.e(v) && !arc; ++i) arc = in_col[i] == p;
+    if (!arc) return 4;
+  }
+  return 0;
+}
+
 // ---- SSSP -------------------------------------------------------------------
 
 // Dijkstra (SSSP.cpp:223-261): ground truth.

@@ -13,7 +13,7 @@ import oracle
 from galois_b200 import assign_weights_u32, rmat, transpose, write_gr
 
 BIN = Path(__file__).resolve().parents[1] / "galois_b200" / "apps" / "bin"
-APPS = ["bfs-gpu", "sssp-gpu", "cc-gpu", "pagerank-gpu", "bc-gpu", "operator-example"]
+APPS = ["bfs-gpu", "bfs-directionopt-gpu", "sssp-gpu", "cc-gpu", "pagerank-gpu", "bc-gpu", "operator-example"]
 
 
 def run(app, *args, check=True):
@@ -90,6 +90,27 @@ def test_bfs_gpu_app(cuda_device, graphs, reorder):
     assert "Verification successful." in p.stdout
     st = stats(p.stdout)
     assert st[("BFS", "Rounds")] >= 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sym", [True, False])
+def test_bfs_directionopt_gpu_app(cuda_device, graphs, tmp_path, sym):
+    d, g, _, src = graphs
+    path = d / "g.gr"
+    if not sym:
+        g, perm = rmat(12, 8, seed=11, symmetrize=False)
+        src = int(perm[0])
+        path = tmp_path / "dir.gr"
+        write_gr(str(path), g, 0)
+    report = int(np.argmax(g.degrees()))
+    args = [path, f"-startNode={src}", f"-reportNode={report}", "-numPrint=5", "-alpha=15", "-beta=18"]
+    p = run("bfs-directionopt-gpu", *args, *(["-symmetricGraph"] if sym else []))
+    want = oracle.bfs_parent_min(g, src, oracle.bfs_serial(g, src))
+    m = re.search(rf"Node {report} has parent (\d+)", p.stdout)
+    assert m and int(m.group(1)) == int(want[report]), p.stdout
+    for v in range(5):
+        assert f"parent[{v}] : {int(want[v])}" in p.stdout
+    assert "Verification successful." in p.stdout
 
 
 @pytest.mark.gpu

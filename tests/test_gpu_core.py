@@ -99,6 +99,44 @@ def test_bfs_device_output_and_errors(cuda_device):
         assert e.value.status == _lib.GB_ERR_ARG
 
 
+# ---- BFS parents (bfsDirectionOpt output) --------------------------------------
+
+@pytest.mark.parametrize("sym,reorder", [(True, 0), (False, 0), (True, 1), (False, 1)])
+def test_bfs_parent_bit_exact(cuda_device, sym, reorder):
+    g, perm = rmat(13, 16, seed=9, symmetrize=sym)
+    src = int(perm[0])
+    lv_want = oracle.bfs_serial(g, src)
+    want = oracle.bfs_parent_min(g, src, lv_want)
+    with DeviceGraph(g, symmetric=sym, reorder=reorder) as dg:
+        # small tiles so the hubs' rows take the tile kernel
+        dg.set_tuning(heavy_degree=32, tile_edges=64)
+        lv = np.empty(g.n, np.uint32)
+        got, st = dg.bfs_parent(src, level_out=lv, stats=True)
+    assert (lv == lv_want).all()
+    assert (got == want).all()
+    assert oracle.verify_bfs_parent(g, src, lv_want, got) == 0
+    assert st["vertices_reached"] == int((lv_want != INF).sum())
+
+
+def test_bfs_parent_small_shapes_and_device_output(cuda_device):
+    import torch
+
+    for g, src in ((path_graph(300), 150), (star_graph(5000), 17), (star_graph(5000), 0),
+                   (HostCSR(np.zeros(1, np.uint64), np.zeros(0, np.uint32)), 0), (grid2d(40, 33), 5)):
+        lv = oracle.bfs_serial(g, src)
+        with DeviceGraph(g, symmetric=True) as dg:
+            out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+            dg.bfs_parent(src, out=out)
+            torch.cuda.synchronize()
+            got = out.cpu().numpy().view(np.uint32)
+        assert (got == oracle.bfs_parent_min(g, src, lv)).all()
+        assert got[src] == 0
+    with DeviceGraph(path_graph(10), symmetric=True) as dg:
+        with pytest.raises(GbError) as e:
+            dg.bfs_parent(10)
+        assert e.value.status == _lib.GB_ERR_ARG
+
+
 # ---- SSSP ---------------------------------------------------------------------
 
 @pytest.mark.parametrize("shift", [0, 5, 13, 31])

@@ -56,6 +56,56 @@ def test_bfs_star_and_isolated():
     assert lv[7] == 0 and lv[0] == 1 and lv[1] == 2
 
 
+def test_bfs_parents_known_answers():
+    # path: every vertex's parent is its predecessor, the source's datum is 0
+    g = path_graph(40)
+    lv = oracle.bfs_serial(g, 10)
+    want = [v + 1 for v in range(10)] + [0] + [v - 1 for v in range(11, 40)]
+    assert oracle.bfs_parent_min(g, 10, lv).tolist() == want
+    assert oracle.bfs_do_parent(g, 10).tolist() == want
+    # star from a leaf: the centre's parent is the leaf, other leaves' the centre
+    g = star_graph(300)
+    lv = oracle.bfs_serial(g, 7)
+    for pa in (oracle.bfs_parent_min(g, 7, lv), oracle.bfs_do_parent(g, 7)):
+        assert pa[7] == 0 and pa[0] == 7
+        assert (np.delete(pa, [0, 7]) == 0).all()
+    # directed path: vertices before the source stay unreached
+    g = path_graph(10, directed=True)
+    pa = oracle.bfs_do_parent(g, 4)
+    assert pa[:4].tolist() == [INF] * 4 and pa[4] == 0 and pa[5:].tolist() == [4, 5, 6, 7, 8]
+
+
+@pytest.mark.parametrize("sym", [True, False])
+def test_bfs_parents_restatements_are_trees(sym):
+    g, perm = rmat(12, 8, seed=5, symmetrize=sym)
+    src = int(perm[0])
+    lv = oracle.bfs_serial(g, src)
+    do = oracle.bfs_do_parent(g, src)
+    pm = oracle.bfs_parent_min(g, src, lv)
+    assert oracle.verify_bfs_parent(g, src, lv, do) == 0
+    assert oracle.verify_bfs_parent(g, src, lv, pm) == 0
+    assert ((do == INF) == (lv == INF)).all()
+    # the min rule is a lower bound of every valid choice
+    reached = (lv != INF) & (np.arange(g.n) != src)
+    assert (pm[reached] <= do[reached]).all()
+
+
+def test_bfs_parent_verifier_catches_planted_mistakes():
+    g, perm = rmat(10, 8, seed=6)
+    src = int(perm[0])
+    lv = oracle.bfs_serial(g, src)
+    pa = oracle.bfs_parent_min(g, src, lv)
+    v = int(np.flatnonzero((lv != INF) & (lv >= 2))[0])
+    bad = pa.copy(); bad[src] = 1
+    assert oracle.verify_bfs_parent(g, src, lv, bad) == 1
+    unreached = np.flatnonzero(lv == INF)
+    if unreached.size:
+        bad = pa.copy(); bad[unreached[0]] = src
+        assert oracle.verify_bfs_parent(g, src, lv, bad) == 2
+    bad = pa.copy(); bad[v] = src  # the source is two or more levels up
+    assert oracle.verify_bfs_parent(g, src, lv, bad) == 3
+
+
 def test_grid_unit_distances_are_manhattan():
     r, c = 17, 23
     g = grid2d(r, c)
