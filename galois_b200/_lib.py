@@ -112,6 +112,9 @@ SIGNATURES: dict[str, tuple] = {
     "gb_graph_device_arrays": (C.c_int, [_gp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
                                          C.POINTER(_vp)]),
     "gb_graph_build_transpose": (C.c_int, [_gp, _vp]),
+    "gb_graph_symmetrize": (C.c_int, [_gp, C.c_int, _vp]),
+    "gb_graph_assign_weights_u32": (C.c_int, [_gp, C.c_uint32, C.c_uint32, C.c_uint64, _vp]),
+    "gb_graph_assign_weights_f32": (C.c_int, [_gp, C.c_uint64, _vp]),
     "gb_graph_reorder": (C.c_int, [_gp, C.c_int, _vp]),
     "gb_pool_trim": (C.c_int, []),
     "gb_graph_permutation": (C.c_int, [_gp, C.POINTER(_vp), C.POINTER(_vp)]),

@@ -136,6 +136,8 @@ int copy_out(void* dst, const void* src_dev, size_t bytes, cudaStream_t stream);
 int copy_in(void* dst_dev, const void* src, size_t bytes, cudaStream_t stream);
 
 int ensure_transpose(gb_graph* g, cudaStream_t stream);
+// Frees every cached array derived from the stored arcs (reorder.cu).
+void drop_derived(gb_graph* g);
 
 // Relabelled graphs (reorder.cu).  result_buf returns the k-th n-word
 // staging buffer (k < 3).  finish_* map a result computed in internal ids

@@ -124,7 +124,11 @@ int blocks_for(const gb_graph* g, uint64_t work) {
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, cap));
 }
 
-// Drop every cached array derived from the old numbering.
+}  // namespace
+
+// Drop every cached array derived from the stored arcs (transpose, sweep
+// schedules, PageRank/PPR state, multi-graph layout): used when the arcs or
+// their numbering change.
 void drop_derived(gb_graph* g) {
   cudaFree(g->t_offs);
   cudaFree(g->t_col);
@@ -156,8 +160,6 @@ void drop_derived(gb_graph* g) {
   g->mg_ngraphs = 0;
   g->mg_hash = 0;
 }
-
-}  // namespace
 
 int reserve_result_bufs(gb_graph* g) {
   if (g->ro_buf) return GB_OK;

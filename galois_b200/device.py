@@ -137,6 +137,53 @@ class DeviceGraph:
     def build_transpose(self) -> None:
         check(lib.gb_graph_build_transpose(self.handle, None), "gb_graph_build_transpose")
 
+    def symmetrize(self, cleanup: bool = True) -> None:
+        """Add every reverse arc on the device (gr2sgr); with cleanup also
+        drop self-loops and repeated arcs (gr2cgr)."""
+        check(lib.gb_graph_symmetrize(self.handle, int(cleanup), None), "gb_graph_symmetrize")
+        self._refresh()
+
+    def assign_weights_u32(self, lo: int, hi: int, seed: int) -> None:
+        """Uniform integer arc weights in [lo, hi], drawn on the device; equal
+        to graph.assign_weights_u32 on the host for the same arcs and seed."""
+        check(lib.gb_graph_assign_weights_u32(self.handle, lo, hi, seed, None), "gb_graph_assign_weights_u32")
+
+    def assign_weights_f32(self, seed: int) -> None:
+        check(lib.gb_graph_assign_weights_f32(self.handle, seed, None), "gb_graph_assign_weights_f32")
+
+    def _refresh(self) -> None:
+        n = C.c_uint32()
+        m = C.c_uint64()
+        s = C.c_int()
+        check(lib.gb_graph_info(self.handle, C.byref(n), C.byref(m), C.byref(s)), "gb_graph_info")
+        self.n, self.m, self.symmetric = n.value, m.value, bool(s.value)
+
+    def to_host(self):
+        """(end_offs, col, w_u32 or None, w_f32 or None) copied back from the
+        device mirror, in its current (possibly relabelled) numbering."""
+        import torch
+
+        a = self.device_arrays()
+        self._refresh()
+
+        class _View:  # a device array seen through __cuda_array_interface__
+            def __init__(self, ptr, count, typestr):
+                self.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr, "data": (ptr, False),
+                                                 "version": 3}
+
+        def grab(ptr, count, dtype):
+            if not ptr:
+                return None
+            if count == 0:
+                return np.empty(0, dtype)
+            signed = {np.uint64: "<i8", np.uint32: "<i4", np.float32: "<f4"}[dtype]
+            t = torch.as_tensor(_View(ptr, count, signed), device=f"cuda:{self.device}")
+            return t.cpu().numpy().view(dtype)
+
+        offs = grab(a["offs"], self.n + 1, np.uint64)
+        return offs[1:].copy(), grab(a["col"], self.m, np.uint32), grab(a["w_u32"], self.m, np.uint32), \
+            grab(a["w_f32"], self.m, np.float32)
+
     def device_arrays(self) -> dict:
         p = [C.c_void_p() for _ in range(4)]
         check(lib.gb_graph_device_arrays(self.handle, *[C.byref(x) for x in p]), "gb_graph_device_arrays")

@@ -153,6 +153,24 @@ int gb_graph_device_arrays(const gb_graph* g, const uint64_t** offs,
  * directed graphs and for the PPR forward pass. */
 int gb_graph_build_transpose(gb_graph* g, void* stream);
 
+/* Conversions applied to the device mirror (tools/graph-convert on a file
+ * in the reference).  gb_graph_symmetrize: gr2sgr (graph-convert.cpp:
+ * 1350-1364, FileGraph.h:764-826): every arc (u,v) with u != v gains the
+ * reverse arc (v,u) with the same weights; with cleanup != 0 it continues as
+ * gr2cgr (Cleanup, graph-convert.cpp:1902-2024), dropping self-loops and
+ * repeated arcs (the first copy in arc order, forward arcs before reverse
+ * ones, keeps its weights).  Rows come out sorted by destination; the graph
+ * is marked symmetric; cached derived arrays are dropped.  Not for a
+ * relabelled graph (call it before gb_graph_reorder); m < 2^31.
+ * gb_graph_assign_weights_u32 / _f32: gr2randomweightgr
+ * (graph-convert.cpp:1169-1190) with the counter-based stream of the host
+ * generators, so the result equals gb_assign_weights_u32 / _f32 on the same
+ * arcs and seed (uniform in [lo, hi]; fp32 in (0, 1]). */
+int gb_graph_symmetrize(gb_graph* g, int cleanup, void* stream);
+int gb_graph_assign_weights_u32(gb_graph* g, uint32_t lo, uint32_t hi,
+                                uint64_t seed, void* stream);
+int gb_graph_assign_weights_f32(gb_graph* g, uint64_t seed, void* stream);
+
 /* Degree-ordered relabelling of the device mirror (no counterpart in the
  * reference, which keeps file order).  GB_ORDER_DEGREE renumbers vertices by
  * descending out-degree (ties by id) and sorts each adjacency list (when

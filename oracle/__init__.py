@@ -155,6 +155,58 @@ def verify_bfs_parent(g, src: int, level, parent) -> int:
     return _lib.orc_verify_bfs_parent(n, _p(in_end), _p(in_col), _p(lv), src, _p(pa))
 
 
+def make_symmetric_file_order(g):
+    """makeSymmetric (libgalois/include/galois/graphs/FileGraph.h:764-826) as
+    the reference writes it: sources ascending, each arc (u, v) appended to
+    u's row and, when u != v, (v, u) with the same edge data appended to v's
+    row, rows filled in that append order.  Returns (end_offs, col, w_u32)."""
+    n, end, col = _g(g)
+    w = None if g.w_u32 is None else np.asarray(g.w_u32, np.uint32)
+    rows = [[] for _ in range(n)]
+    b = 0
+    for u in range(n):
+        e = int(end[u])
+        for i in range(b, e):
+            v = int(col[i])
+            data = None if w is None else int(w[i])
+            rows[u].append((v, data))
+            if u != v:
+                rows[v].append((u, data))
+        b = e
+    out_col = np.array([v for r in rows for v, _ in r], np.uint32)
+    out_w = None if w is None else np.array([d for r in rows for _, d in r], np.uint32)
+    out_end = np.cumsum([len(r) for r in rows], dtype=np.uint64)
+    return out_end, out_col, out_w
+
+
+def make_symmetric(g, cleanup: bool):
+    """The device form of gr2sgr (and gr2cgr with cleanup): the arcs of
+    make_symmetric_file_order with every row sorted by destination, forward
+    copies before reverse ones and earlier arcs first among equal
+    destinations; with cleanup (Cleanup, tools/graph-convert/
+    graph-convert.cpp:1902-2024) self-loops dropped and, of repeated arcs,
+    the first kept.  Returns (end_offs, col, w_u32)."""
+    n, end, col = _g(g)
+    m = col.size
+    deg = np.diff(np.concatenate(([0], end.astype(np.int64))))
+    src = np.repeat(np.arange(n, dtype=np.uint64), deg)
+    dst = col.astype(np.uint64)
+    idx = np.arange(m, dtype=np.int64)
+    rev = dst != src
+    s_all = np.concatenate([src, dst[rev]])
+    d_all = np.concatenate([dst, src[rev]])
+    i_all = np.concatenate([idx, idx[rev]])
+    order = np.argsort((s_all << np.uint64(32)) | d_all, kind="stable")
+    s_all, d_all, i_all = s_all[order], d_all[order], i_all[order]
+    if cleanup and s_all.size:
+        keep = s_all != d_all
+        keep[1:] &= (s_all[1:] != s_all[:-1]) | (d_all[1:] != d_all[:-1])
+        s_all, d_all, i_all = s_all[keep], d_all[keep], i_all[keep]
+    out_end = np.cumsum(np.bincount(s_all.astype(np.int64), minlength=n), dtype=np.uint64)
+    out_w = None if g.w_u32 is None else np.asarray(g.w_u32, np.uint32)[i_all]
+    return out_end, d_all.astype(np.uint32), out_w
+
+
 def sssp_dijkstra(g, src: int) -> np.ndarray:
     n, end, col = _g(g)
     w = np.ascontiguousarray(g.w_u32, np.uint32)

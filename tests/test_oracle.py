@@ -106,6 +106,46 @@ def test_bfs_parent_verifier_catches_planted_mistakes():
     assert oracle.verify_bfs_parent(g, src, lv, bad) == 3
 
 
+def _rows(end, col, w):
+    out, b = [], 0
+    for e in end:
+        out.append(sorted(zip(col[b:e].tolist(), [] if w is None else w[b:e].tolist()) if w is not None
+                          else col[b:e].tolist()))
+        b = int(e)
+    return out
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_make_symmetric_rows_match_reference_order(seed):
+    # random multigraph with self-loops: the sorted device form holds, row by
+    # row, the same arcs and weights as makeSymmetric's append order
+    rng = np.random.default_rng(seed)
+    n, m = 40, 300
+    g = HostCSR.from_edges(n, rng.integers(0, n, m), rng.integers(0, n, m), w_u32=rng.integers(1, 9, m))
+    ref = oracle.make_symmetric_file_order(g)
+    got = oracle.make_symmetric(g, cleanup=False)
+    assert np.array_equal(ref[0], got[0])
+    assert _rows(*ref) == _rows(*got)
+    loops = int((np.repeat(np.arange(n), g.degrees()) == g.col).sum())
+    assert got[1].size == 2 * m - loops
+
+
+def test_make_symmetric_cleanup_known_answers():
+    g = HostCSR.from_edges(4, [0, 0, 1, 2, 3, 3], [1, 1, 1, 3, 2, 0], w_u32=[5, 6, 7, 8, 9, 4])
+    end, col, w = oracle.make_symmetric(g, cleanup=True)
+    # 0-1 once (first copy, weight 5), self-loop 1-1 gone, 3-0 once (weight
+    # 4); 2-3 and 3-2 are both stored arcs, so each row keeps its own
+    # forward copy (8 in row 2, 9 in row 3) over the other's reverse copy
+    assert end.tolist() == [2, 3, 4, 6]
+    assert col.tolist() == [1, 3, 0, 3, 0, 2]
+    assert w.tolist() == [5, 4, 5, 8, 4, 9]
+    # symmetrising the directed generator output gives the symmetric one
+    gd, _ = rmat(10, 8, seed=4, symmetrize=False)
+    gs, _ = rmat(10, 8, seed=4, symmetrize=True)
+    end, col, _ = oracle.make_symmetric(gd, cleanup=True)
+    assert np.array_equal(end, gs.end_offs) and np.array_equal(col, gs.col)
+
+
 def test_grid_unit_distances_are_manhattan():
     r, c = 17, 23
     g = grid2d(r, c)
