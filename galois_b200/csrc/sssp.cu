@@ -23,7 +23,7 @@
 //   * a far pile holding vertices relaxed beyond the bucket (membership
 //     bitmap, so each vertex is in the pile at most once);
 //   * for large frontiers, a bitmap instead of the near queue: a phase whose
-//     input frontier is estimated above `bm_min` relaxes with reductions
+//     input frontier is estimated above `bm_min` arcs relaxes with reductions
 //     that return nothing (red.min on the distance, red.or on the next
 //     phase's bitmap), so a warp step never waits on an atomic's reply, and
 //     the next phase sweeps the bitmap in id order (light rows 1024 ids per
@@ -184,7 +184,9 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
     if (kBitmap && bm_in ? bm_count != 0 : (q_light != 0 || q_tiles != 0)) {
       // ---- relaxation phase --------------------------------------------
       // every thread reads the same counters, so the choice is grid-uniform
-      const uint64_t est = bm_in ? (uint64_t)bm_count : (uint64_t)q_light + 8ull * q_tiles;
+      // estimated arcs of the input frontier (a light vertex counted as 16
+      // arcs, a tile as its width): the arcs bound the vertices it can reach
+      const uint64_t est = bm_in ? 16ull * bm_count : 16ull * q_light + (uint64_t)a.tile * q_tiles;
       const bool bm_out = kBitmap && est > a.bm_min;
       uint32_t* const act_next = a.act[(P + 1) % 3];
       uint32_t my_push = 0;  // lane 0: this warp's bit-setting reductions
@@ -558,10 +560,11 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   a.all_light = g->max_degree <= t.heavy_degree ? 1 : 0;
   a.sw_tiles = sched.tiles;
   a.sw_ntiles = sched.ntiles;
-  // a frontier of more than n/64 vertices (a tile counting as 8) makes the
-  // next one a bitmap: its sweep reads n/8 bytes of bitmap, small beside the
-  // arcs of such a frontier
-  a.bm_min = n >> 6;
+  // a frontier estimated at more than n/256 arcs writes the next one as a
+  // bitmap: its sweep reads n/8 bytes of bitmap and the tile schedule, small
+  // beside what such a frontier relaxes (n/64 and n/1024 measured slower on
+  // RMAT-22/24)
+  a.bm_min = n >> 8;
   GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), s));
   sssp_init<<<g->sm_count * 4, 256, 0, s>>>(a);
   GB_CUDA(cudaGetLastError());
