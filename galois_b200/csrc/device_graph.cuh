@@ -34,8 +34,10 @@ struct gb_graph {
   uint64_t* t_emap = nullptr;
   // cached per-graph derived arrays
   uint32_t* outdeg_of_stored = nullptr;  // PageRank nout (in-degree counts of the stored graph)
-  // degree-ordered graphs: row id of every arc of the light rows
-  // [lr_row0, zero_from), arcs [lr_arc0, lr_arc1), for flat pull sweeps
+  // degree-ordered graphs: the rows of the light rows' arcs [lr_arc0,
+  // lr_arc1) (rows [lr_row0, zero_from)) for flat pull sweeps, packed as the
+  // first row of every 256-arc run (uint32) followed by each arc's row offset
+  // from its run's first row (one byte)
   uint32_t* lr_rowid = nullptr;
   uint32_t lr_row0 = 0, lr_heavy = 0;
   uint64_t lr_arc0 = 0, lr_arc1 = 0;

@@ -81,11 +81,16 @@ struct PrArgs {
   FrontierQueues fq;
   uint32_t heavy, tile;
   uint32_t zero_from;  // first vertex of the no-in-arc suffix (degree-ordered graphs), else n
-  // flat sweep of the light rows (degree-ordered graphs): arcs [lr_arc0, lr_arc1)
-  // with their row ids
-  const uint32_t* __restrict__ lr_rowid;
+  // flat sweep of the light rows (degree-ordered graphs): arcs [lr_arc0,
+  // lr_arc1) in runs of kLightRun; an arc's row is lr_runrow[run] +
+  // lr_rowd[arc - lr_arc0] (a run spans at most kLightRun rows, so the
+  // offset fits a byte: a quarter of the bytes of a row id per arc)
+  const uint32_t* __restrict__ lr_runrow;
+  const uint8_t* __restrict__ lr_rowd;
   uint64_t lr_arc0, lr_arc1;
 };
+
+constexpr int kLightRun = 256;  // arcs per light-row run of pr_pull_flat (32 lanes x 8)
 
 __global__ void count_nout(const uint32_t* __restrict__ col, uint64_t m, uint32_t* nout) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -352,15 +357,18 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
         sum = warp_sum(sum);
         if (lane == 0) atomicAdd(&acc_cur[tv.x], sum);
       } else {
-        // 256 arcs of the light rows
-        const uint64_t r0 = a.lr_arc0 + (t - a.sched.ntiles) * (32 * UT);
+        // one run of 256 arcs of the light rows
+        static_assert(32 * UT == kLightRun, "a light run is one warp step of UT arcs per lane");
+        const uint64_t run = t - a.sched.ntiles;
+        const uint64_t r0 = a.lr_arc0 + run * kLightRun;
+        const uint32_t row0 = ldg(a.lr_runrow + run);
         uint32_t u[UT], row[UT];
 #pragma unroll
         for (int k = 0; k < UT; ++k) {
           const uint64_t i = r0 + lane + 32 * k;
           const bool ok = i < a.lr_arc1;
           u[k] = ok ? ldg(a.col + i) : 0u;
-          row[k] = ok ? ldg(a.lr_rowid + (i - a.lr_arc0)) : 0xFFFFFFFFu;
+          row[k] = ok ? row0 + (uint32_t)__ldg(a.lr_rowd + (i - a.lr_arc0)) : 0xFFFFFFFFu;
         }
         float x[UT];
 #pragma unroll
@@ -394,11 +402,24 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
   }
 }
 
-__global__ void light_rowid_kernel(const uint64_t* __restrict__ offs, uint32_t row0, uint32_t row1, uint64_t arc0,
-                                   uint32_t* __restrict__ rowid) {
+// The light rows' run table, in two passes: the row holding each run's first
+// arc, then every arc's offset from it.
+__global__ void light_runrow_kernel(const uint64_t* __restrict__ offs, uint32_t row0, uint32_t row1, uint64_t arc0,
+                                    uint32_t* __restrict__ runrow) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = row0 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < row1; v += stride) {
+    const uint64_t b = offs[v] - arc0, e = offs[v + 1] - arc0;
+    // the runs whose first arc lies in [b, e)
+    for (uint64_t r = (b + kLightRun - 1) / kLightRun; r * kLightRun < e; ++r) runrow[r] = (uint32_t)v;
+  }
+}
+
+__global__ void light_rowd_kernel(const uint64_t* __restrict__ offs, uint32_t row0, uint32_t row1, uint64_t arc0,
+                                  const uint32_t* __restrict__ runrow, uint8_t* __restrict__ rowd) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t v = row0 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < row1; v += stride)
-    for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) rowid[e - arc0] = (uint32_t)v;
+    for (uint64_t e = offs[v] - arc0; e < offs[v + 1] - arc0; ++e)
+      rowd[e] = (uint8_t)((uint32_t)v - runrow[e / kLightRun]);
 }
 
 // ---- pull-residual (PageRank-pull.cpp:132-190) ------------------------------
@@ -683,16 +704,26 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
         GB_CUDA(cudaMemcpyAsync(&ends[1], g->offs + g->zero_from, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         GB_CUDA(cudaStreamSynchronize(s));
         if (ends[1] < ends[0]) GB_FAIL(GB_ERR_CUDA, "pagerank: light rows out of order");
-        GB_CUDA(cudaMalloc(&g->lr_rowid, sizeof(uint32_t) * std::max<uint64_t>(ends[1] - ends[0], 1)));
-        if (g->zero_from > sched.nheavy)
-          light_rowid_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, sched.nheavy, g->zero_from, ends[0], g->lr_rowid);
+        // one allocation: the run rows (uint32 per run), then a byte per arc
+        const uint64_t narcs = ends[1] - ends[0];
+        const uint64_t nruns = (narcs + kLightRun - 1) / kLightRun;
+        GB_CUDA(cudaMalloc(&g->lr_rowid, sizeof(uint32_t) * std::max<uint64_t>(nruns, 1) + narcs + 16));
+        if (g->zero_from > sched.nheavy) {
+          uint32_t* runrow = g->lr_rowid;
+          uint8_t* rowd = reinterpret_cast<uint8_t*>(g->lr_rowid + std::max<uint64_t>(nruns, 1));
+          light_runrow_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, sched.nheavy, g->zero_from, ends[0], runrow);
+          light_rowd_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, sched.nheavy, g->zero_from, ends[0], runrow,
+                                                              rowd);
+        }
         GB_CUDA(cudaGetLastError());
         g->lr_row0 = sched.nheavy;
         g->lr_heavy = sched.heavy;
         g->lr_arc0 = ends[0];
         g->lr_arc1 = ends[1];
       }
-      a.lr_rowid = g->lr_rowid;
+      a.lr_runrow = g->lr_rowid;
+      a.lr_rowd = reinterpret_cast<const uint8_t*>(
+          g->lr_rowid + std::max<uint64_t>((g->lr_arc1 - g->lr_arc0 + kLightRun - 1) / kLightRun, 1));
       a.lr_arc0 = g->lr_arc0;
       a.lr_arc1 = g->lr_arc1;
       kfn = reinterpret_cast<const void*>(&pr_pull_flat<kBlock, 6>);
