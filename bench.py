@@ -145,12 +145,13 @@ class ClockSampler:
         except Exception:
             pass
 
-    def _nvml_loop(self, stop, rows):
+    def _nvml_loop(self, stop, rows, ready):
         try:
             import pynvml as nv
 
             nv.nvmlInit()
         except Exception:
+            ready.set()
             return
         try:
             h = nv.nvmlDeviceGetHandleByUUID(self.uuid) if self.uuid else nv.nvmlDeviceGetHandleByIndex(self.gpu)
@@ -161,10 +162,12 @@ class ClockSampler:
                 sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
                 mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
                 rows.append((sm, smax, tuple(bool(mask & b) for b in bits)))
+                ready.set()
                 stop.wait(self.period_s)
         except Exception:
             pass
         finally:
+            ready.set()
             try:
                 nv.nvmlShutdown()
             except Exception:
@@ -181,8 +184,13 @@ class ClockSampler:
             self.proc = None
         self._stop = threading.Event()
         self._nvml_rows = []
-        self.thread = threading.Thread(target=self._nvml_loop, args=(self._stop, self._nvml_rows), daemon=True)
+        ready = threading.Event()
+        self.thread = threading.Thread(target=self._nvml_loop, args=(self._stop, self._nvml_rows, ready), daemon=True)
         self.thread.start()
+        # the timed region starts only once NVML is sampling (bounded wait);
+        # the samples taken before it are dropped
+        ready.wait(2.0)
+        self._t0 = len(self._nvml_rows)
 
     def stop(self) -> dict:
         if self.thread is not None:
@@ -202,7 +210,9 @@ class ClockSampler:
                     rows.append((float(r[1]), float(r[2]), tuple(r[5 + i].lower() == "active" for i in range(4))))
         os.unlink(self.file.name)
         n_smi = len(rows)
-        rows += self._nvml_rows if self.thread is not None else []
+        if self.thread is not None:
+            # a region shorter than one period keeps the sample taken as it began
+            rows += self._nvml_rows[self._t0:] or self._nvml_rows[-1:]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [] if self.proc else ["nvidia-smi unavailable"],
                     "samples": 0}
@@ -875,14 +885,20 @@ def main() -> None:
                     job.device_call(dg, gi, host_out[gi])
 
         e2e_step()
-        ke = max(1, min(args.steps, 5))
+        ke = max(1, min(args.steps, 10))
         dist.barrier()
         t0 = time.perf_counter()
+        step_ms = []
         for _ in range(ke):
+            ts = time.perf_counter()
             e2e_step()
+            step_ms.append(round((time.perf_counter() - ts) * 1e3, 2))
         te = dist.max(time.perf_counter() - t0)
         line["e2e"] = {"value": aggregate_rate(dist.world, units_step, ke, te * 1e3), "unit": job.unit,
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": ke,
+                       # every step's wall time on this rank: the host-to-device copy rate of a shared
+                       # host varies from step to step, and value is over all of them
+                       "step_ms": step_ms,
                        "path": "gb_graph_upload (pinned host CSR, file order: a one-shot call does not "
                                "amortise gb_graph_reorder) + kernel + host output copy + gb_graph_free"}
     for dg in dgs:
