@@ -39,7 +39,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--app", choices=["sssp", "bfs", "cc", "pr", "bc", "multigraph", "ppr"], default="sssp")
+    ap.add_argument("--app", choices=["sssp", "bfs", "cc", "pr", "pr-residual", "bc", "multigraph", "ppr"], default="sssp")
     ap.add_argument("--size", choices=["small", "medium", "full", "s24"], default="full",
                     help="graph sizes: full = the benchmark configuration; s24 = RMAT scale 24 for every "
                          "app; medium/small for profiling")
@@ -394,6 +394,12 @@ class CcJob(Job):
         g, _ = rmat(scale, 16, seed=24, symmetrize=True)
         self.graphs.append({"name": f"rmat{scale}-sym", "host": g, "symmetric": True, "src": 0})
 
+    def cpu_run(self, g):
+        """(output, units) of the CPU restatement on host graph g."""
+        import oracle
+
+        return oracle.cc_labelprop(g)[0], float(g.m)
+
     def device_call(self, dg, gi, out):
         dg.cc(0, out=out)
 
@@ -451,17 +457,49 @@ class PrJob(Job):
         g = self.graphs[gi]["host"]
         return st["iterations"] * (8.0 * g.m + 24.0 * g.n)
 
-    def cpu_call(self, gi):
+    def cpu_run(self, g):
+        """(output, units) of the CPU restatement on host graph g."""
         import oracle
 
-        return oracle.pr_pull_topo_par(self.graphs[gi]["host"], 0.85, 1e-6, 1000)[0]
+        x, it = oracle.pr_pull_topo_par(g, 0.85, 1e-6, 1000)
+        return x, float(it) * g.m
+
+    def cpu_call(self, gi):
+        return self.cpu_run(self.graphs[gi]["host"])[0]
 
     def parity(self, gpu_out, cpu_out, gi):
         err = float(np.abs(gpu_out.view(np.float32).astype(np.float64) - cpu_out).max())
         return f"max abs diff vs CPU fp32 in-place {err:.2e}"
 
 
-JOBS = {"sssp": SsspJob, "bfs": BfsJob, "cc": CcJob, "pr": PrJob}
+class PrResidualJob(PrJob):
+    """PageRank pull-residual (PageRank-pull.cpp:132-190), the app's default
+    -algo, at its default tolerance 1e-3 (PageRank-constants.h)."""
+
+    kernel = "pr_pull_residual_persistent"
+    workload = "PageRank pull-residual, alpha 0.85, tol 1e-3 (per vertex), max 1000, RMAT-24 symmetric ef16"
+    tol = 1e-3
+
+    def device_call(self, dg, gi, out):
+        dg.pagerank_pull_residual(0.85, self.tol, 1000, out=out)
+
+    def stats_call(self, dg, gi, out):
+        st = dg.pagerank_pull_residual(0.85, self.tol, 1000, out=out, stats=True)[1]
+        self.iters[gi] = st["iterations"]
+        return st
+
+    def cpu_run(self, g):
+        import oracle
+
+        x, it = oracle.pr_pull_residual(g, 0.85, self.tol, 1000, f64=False)
+        return x, float(it) * g.m
+
+    def parity(self, gpu_out, cpu_out, gi):
+        err = float(np.abs(gpu_out.view(np.float32).astype(np.float64) - cpu_out).max())
+        return f"max abs diff vs CPU fp32 restatement {err:.2e}"
+
+
+JOBS = {"sssp": SsspJob, "bfs": BfsJob, "cc": CcJob, "pr": PrJob, "pr-residual": PrResidualJob}
 ORDER_NAMES = {0: "file order", 1: "degree-ordered (gb_graph_reorder, sorted rows)",
                2: "degree-ordered (gb_graph_reorder, unsorted rows)"}
 BATCHED = ("bc", "multigraph", "ppr")
@@ -714,19 +752,17 @@ def run_reference(args, job_cls) -> None:
     job = job_cls(args.size)
     # units per step: the same traversed-edge count the GPU arm reports,
     # computed on the host from the CPU result (reached vertices' degrees)
+    # the first (untimed) pass is also the first warm-up step
     t0 = time.perf_counter()
-    outs = [job.cpu_call(gi) for gi in range(len(job.graphs))]
-    first = time.perf_counter() - t0
     units = 0.0
-    for gi, out in enumerate(outs):
+    for gi in range(len(job.graphs)):
         g = job.graphs[gi]["host"]
         if isinstance(job, (SsspJob, BfsJob)):
+            out = job.cpu_call(gi)
             units += float(g.degrees()[np.asarray(out) != oracle.INF].sum())
-        elif isinstance(job, CcJob):
-            units += float(g.m)
         else:
-            _, it = oracle.pr_pull_topo_par(g, 0.85, 1e-6, 1000)
-            units += float(it) * g.m
+            units += job.cpu_run(g)[1]
+    first = time.perf_counter() - t0
     steps, warm = args.steps, args.warmup
     if first * (steps + warm) > 240.0:  # keep the whole arm within a few minutes
         steps, warm = max(1, int(240.0 / max(first, 1e-3)) - 1), 1
@@ -823,7 +859,7 @@ def main() -> None:
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_src,
                 # a degree-ordered PageRank runs the flat pull kernel
-                "kernel": "pr_pull_flat" if (isinstance(job, PrJob) and args.order) else job.kernel,
+                "kernel": "pr_pull_flat" if (type(job) is PrJob and args.order) else job.kernel,
                 "algorithmic_bytes_per_step": bytes_step, "kernel_ms_per_step": sum(kms),
                 # the same over the arcs the kernel actually read
                 "work_bytes_per_step": work_step,
@@ -848,12 +884,7 @@ def main() -> None:
 
             gs, _ = rmat(22, 16, seed=24, symmetrize=True)
             t0 = time.perf_counter()
-            if isinstance(job, CcJob):
-                oracle.cc_labelprop(gs)
-                cu = float(gs.m)
-            else:
-                _, it = oracle.pr_pull_topo_par(gs, 0.85, 1e-6, 1000)
-                cu = float(it) * gs.m
+            _, cu = job.cpu_run(gs)
             t_cpu = time.perf_counter() - t0
             line["cpu_baseline"] = {"value": cu / t_cpu / 1e9, "unit": job.unit, "cores": oracle.threads(),
                                     "kind": "port", "sample": "same algorithm on RMAT-22 sym ef16 (bounded sample)"}
