@@ -39,7 +39,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--app", choices=["sssp", "bfs", "cc", "pr", "pr-residual", "bc", "multigraph", "ppr"], default="sssp")
+    ap.add_argument("--app", choices=["sssp", "bfs", "bfs-parent", "cc", "pr", "pr-residual", "bc", "multigraph", "ppr"], default="sssp")
     ap.add_argument("--size", choices=["small", "medium", "full", "s24"], default="full",
                     help="graph sizes: full = the benchmark configuration; s24 = RMAT scale 24 for every "
                          "app; medium/small for profiling")
@@ -382,6 +382,50 @@ class BfsJob(Job):
         return oracle.bfs_sync_tile(g["host"], g["src"])
 
 
+class BfsParentJob(BfsJob):
+    """BFS with parents (bfsDirectionOpt's output): the BFS kernel, then the
+    parent pass over every in-arc (gb_bfs_parent)."""
+
+    kernel = "bfs_persistent + parent_rows/parent_tiles"
+    workload = "BFS parents (smallest-id valid parent) from the max-degree vertex, RMAT-20 symmetric ef16"
+    cpu_serial = True  # the restatement of SyncDO is serial
+
+    def __init__(self, size):
+        super().__init__(size)
+
+    def device_call(self, dg, gi, out):
+        dg.bfs_parent(self.graphs[gi]["src"], out=out)
+
+    def stats_call(self, dg, gi, out):
+        return dg.bfs_parent(self.graphs[gi]["src"], out=out, stats=True)[1]
+
+    def algo_bytes(self, st, gi):
+        # the BFS push model, then column + level per in-arc and offsets, level
+        # and parent per vertex for the parent pass
+        g = self.graphs[gi]["host"]
+        return super().algo_bytes(st, gi) + 8.0 * g.m + 24.0 * g.n
+
+    def work_bytes(self, st, gi):
+        g = self.graphs[gi]["host"]
+        return super().work_bytes(st, gi) + 8.0 * g.m + 24.0 * g.n
+
+    def cpu_call(self, gi):
+        import oracle
+
+        g = self.graphs[gi]
+        return oracle.bfs_do_parent(g["host"], g["src"])
+
+    def parity(self, gpu_out, cpu_out, gi):
+        import oracle
+
+        g = self.graphs[gi]
+        lv = oracle.bfs_serial(g["host"], g["src"])
+        got = gpu_out.view(np.uint32)
+        same = np.array_equal(got, oracle.bfs_parent_min(g["host"], g["src"], lv))
+        ok = oracle.verify_bfs_parent(g["host"], g["src"], lv, got) == 0
+        return f"{'bit-exact' if same else 'MISMATCH'} vs the min-id rule; BFS tree {'valid' if ok else 'INVALID'}"
+
+
 class CcJob(Job):
     kernel = "cc_labelprop"
     workload = "CC label propagation + pointer jumping, RMAT-24 symmetric ef16, min-id labels"
@@ -499,7 +543,7 @@ class PrResidualJob(PrJob):
         return f"max abs diff vs CPU fp32 restatement {err:.2e}"
 
 
-JOBS = {"sssp": SsspJob, "bfs": BfsJob, "cc": CcJob, "pr": PrJob, "pr-residual": PrResidualJob}
+JOBS = {"sssp": SsspJob, "bfs": BfsJob, "bfs-parent": BfsParentJob, "cc": CcJob, "pr": PrJob, "pr-residual": PrResidualJob}
 ORDER_NAMES = {0: "file order", 1: "degree-ordered (gb_graph_reorder, sorted rows)",
                2: "degree-ordered (gb_graph_reorder, unsorted rows)"}
 BATCHED = ("bc", "multigraph", "ppr")
@@ -777,7 +821,7 @@ def run_reference(args, job_cls) -> None:
         times.append(time.perf_counter() - t0)
     t = sum(times)
     value = units * steps / t / 1e9
-    cores = oracle.threads()
+    cores = 1 if getattr(job, "cpu_serial", False) else oracle.threads()
     sample = f"full workload per step ({steps} timed steps, {warm} warm-up)"
     emit({"impl": "reference", "metric": job.metric, "value": value, "unit": job.unit, "n_gpus": args.gpus,
           "steps": steps, "warmup": warm, "ms_per_step": 1e3 * t / steps, "higher_is_better": True,
@@ -893,7 +937,8 @@ def main() -> None:
             cpu_outs = [job.cpu_call(gi) for gi in range(len(job.graphs))]
             t_cpu = time.perf_counter() - t0
             gpu_host = [o.cpu().numpy() for o in outs]
-            line["cpu_baseline"] = {"value": units_step / t_cpu / 1e9, "unit": job.unit, "cores": oracle.threads(),
+            line["cpu_baseline"] = {"value": units_step / t_cpu / 1e9, "unit": job.unit,
+                                    "cores": 1 if getattr(job, "cpu_serial", False) else oracle.threads(),
                                     "kind": "port", "sample": "one full run of every graph of the workload",
                                     "parity": [job.parity(gpu_host[gi], cpu_outs[gi], gi)
                                                for gi in range(len(job.graphs))]}

@@ -148,11 +148,13 @@ extern "C" int gb_bfs_parent(gb_graph* g, uint32_t src, uint32_t* parent_out, ui
     sched.ntiles = ntiles;
   }
   const int grid = g->sm_count * 8;
+  KernelTimer kt(stats != nullptr, s);  // the parent pass, added to the BFS kernel time
   parent_rows<kParentBlock><<<grid, kParentBlock, 0, s>>>(in_offs, in_col, lvl, g->perm, n, t.heavy_degree, par);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess && sched.ntiles)
     parent_tiles<<<grid, 256, 0, s>>>(in_offs, in_col, lvl, g->perm, sched.tiles, sched.ntiles, t.tile_edges, par);
   if (e == cudaSuccess) e = cudaGetLastError();
+  kt.stop(s);
   if (tiles) {
     // the tiles must outlive the launch that reads them
     const cudaError_t se = cudaStreamSynchronize(s);
@@ -161,7 +163,11 @@ extern "C" int gb_bfs_parent(gb_graph* g, uint32_t src, uint32_t* parent_out, ui
     cudaFree(heavy_list);
   }
   if (e != cudaSuccess) return cuda_fail(e, "gb_bfs_parent");
-  if (stats) stats->launches += sched.ntiles ? 2 : 1;
+  if (stats) {
+    GB_CUDA(cudaStreamSynchronize(s));
+    stats->launches += sched.ntiles ? 2 : 1;
+    stats->kernel_ms += kt.ms();
+  }
   if (g->perm) {
     if (level_out) {
       st = finish_u32(g, lvl, level_out, s);
