@@ -28,12 +28,11 @@ def test_cpu_run_units():
 
     b = _bench()
     g, _ = rmat(10, 8, seed=3, symmetrize=True)
-    x, units = b.PrJob.__new__(b.PrJob).cpu_run(g)
-    _, it = oracle.pr_pull_topo_par(g, 0.85, 1e-6, 1000)
-    assert units == it * g.m and x.shape == (g.n,)
-    x, units = b.PrResidualJob.__new__(b.PrResidualJob).cpu_run(g)
-    _, it = oracle.pr_pull_residual(g, 0.85, 1e-3, 1000, f64=False)
-    assert units == it * g.m and x.shape == (g.n,)
+    # PageRank units are whole sweeps of the arcs (the parallel restatements
+    # update in place, so their round count depends on the thread count)
+    for cls in (b.PrJob, b.PrResidualJob):
+        x, units = cls.__new__(cls).cpu_run(g)
+        assert units > 0 and units % g.m == 0 and x.shape == (g.n,)
     lab, units = b.CcJob.__new__(b.CcJob).cpu_run(g)
     assert units == g.m and np.array_equal(lab, oracle.cc_union_find(g))
 
