@@ -9,6 +9,10 @@ on each graph.  Metric: GTEPS = (m_r(a) + m_r(b)) / step time, m_r = arcs out
 of reached vertices.  Other --app values run the other hot-path kernels on
 their configurations (bfs: RMAT-20 sym; cc, pr: RMAT-24 sym).
 
+On one GPU the default run also measures BFS (RMAT-20 and RMAT-24), CC and
+PageRank pull-topological (RMAT-24) and reports them under "apps", each with
+its parity against the oracle.
+
 Prints ONE JSON line (rank 0).  `--impl reference` times the CPU restatement of
 the reference algorithm (oracle/, OpenMP on all host cores) on the same
 workload instead.
@@ -49,6 +53,8 @@ def parse_args():
     ap.add_argument("--small", action="store_true", help="same as --size small")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-apps", action="store_true",
+                    help="skip the BFS / CC / PageRank configurations that the default run adds under 'apps'")
     args = ap.parse_args()
     if args.small:
         args.size = "small"
@@ -278,6 +284,10 @@ class Job:
         self.size = size
         self.graphs = []  # dicts: name, host (HostCSR), symmetric, src
 
+    def check(self, gpu_out: np.ndarray, gi: int) -> str:
+        """Parity of one GPU output against the oracle's ground truth."""
+        raise NotImplementedError
+
     def device_call(self, dg, gi, out):
         raise NotImplementedError
 
@@ -313,6 +323,12 @@ class Job:
 
 
 class SsspJob(Job):
+    # the oracle's delta-stepping drains the current bucket in parallel rounds
+    # before it opens the next one
+    CPU_SCHEDULE = ("bucket-synchronous delta-stepping (OBIM with a barrier between buckets): the schedule the "
+                    "reference's Auto choice runs on the grid (deltaStepBarrier, SSSP.cpp:410-416,453); on the "
+                    "power-law RMAT graph the reference picks barrier-free OBIM (deltaStep), which this "
+                    "restatement does not model")
     kernel = "sssp_persistent"
     workload = "SSSP delta-stepping, delta=2^13, w~U[1,255]: RMAT-22 directed ef16 (src = generator vertex 0) + grid 4096x4096 (src 0)"
 
@@ -353,15 +369,24 @@ class BfsJob(Job):
     kernel = "bfs_persistent"
     workload = "BFS from the max-degree vertex, RMAT-20 symmetric ef16"
 
-    def __init__(self, size):
+    def __init__(self, size, graph=None, name=None):
         super().__init__(size)
         from galois_b200 import rmat
 
-        scale = pick(size, 16, 21, 20, 24)
-        self.workload = self.workload.replace("RMAT-20", f"RMAT-{scale}")
-        g, _ = rmat(scale, 16, seed=20, symmetrize=True)
-        self.graphs.append({"name": f"rmat{scale}-sym", "host": g, "symmetric": True,
-                            "src": int(np.argmax(g.degrees()))})
+        if graph is None:
+            scale = pick(size, 16, 21, 20, 24)
+            graph, _ = rmat(scale, 16, seed=20, symmetrize=True)
+            name = f"rmat{scale}-sym"
+        self.workload = self.workload.replace("RMAT-20", name.split("-")[0].upper().replace("RMAT", "RMAT-"))
+        self.graphs.append({"name": name, "host": graph, "symmetric": True,
+                            "src": int(np.argmax(graph.degrees()))})
+
+    def check(self, gpu_out, gi):
+        import oracle
+
+        g = self.graphs[gi]
+        same = np.array_equal(gpu_out.view(np.uint32), oracle.bfs_serial(g["host"], g["src"]))
+        return "bit-exact vs the oracle's serial BFS" if same else "MISMATCH vs the oracle's serial BFS"
 
     def device_call(self, dg, gi, out):
         dg.bfs(self.graphs[gi]["src"], out=out)
@@ -425,18 +450,29 @@ class BfsParentJob(BfsJob):
         ok = oracle.verify_bfs_parent(g["host"], g["src"], lv, got) == 0
         return f"{'bit-exact' if same else 'MISMATCH'} vs the min-id rule; BFS tree {'valid' if ok else 'INVALID'}"
 
+    def check(self, gpu_out, gi):
+        return self.parity(gpu_out, None, gi)
+
 
 class CcJob(Job):
     kernel = "cc_labelprop"
     workload = "CC label propagation + pointer jumping, RMAT-24 symmetric ef16, min-id labels"
 
-    def __init__(self, size):
+    def __init__(self, size, graph=None, name=None):
         super().__init__(size)
         from galois_b200 import rmat
 
-        scale = pick(size, 18, 21, 24)
-        g, _ = rmat(scale, 16, seed=24, symmetrize=True)
-        self.graphs.append({"name": f"rmat{scale}-sym", "host": g, "symmetric": True, "src": 0})
+        if graph is None:
+            scale = pick(size, 18, 21, 24)
+            graph, _ = rmat(scale, 16, seed=24, symmetrize=True)
+            name = f"rmat{scale}-sym"
+        self.graphs.append({"name": name, "host": graph, "symmetric": True, "src": 0})
+
+    def check(self, gpu_out, gi):
+        import oracle
+
+        same = np.array_equal(gpu_out.view(np.uint32), oracle.cc_union_find(self.graphs[gi]["host"]))
+        return "bit-exact vs the oracle's union-find min-id labels" if same else "MISMATCH vs union-find labels"
 
     def cpu_run(self, g):
         """(output, units) of the CPU restatement on host graph g."""
@@ -474,14 +510,25 @@ class PrJob(Job):
     dtype = "f32"
     workload = "PageRank pull-topological, alpha 0.85, tol 1e-6 (L1), max 1000, RMAT-24 symmetric ef16"
 
-    def __init__(self, size):
+    def __init__(self, size, graph=None, name=None):
         super().__init__(size)
         from galois_b200 import rmat
 
-        scale = pick(size, 18, 21, 24)
-        g, _ = rmat(scale, 16, seed=24, symmetrize=True)
-        self.graphs.append({"name": f"rmat{scale}-sym", "host": g, "symmetric": True, "src": 0})
+        if graph is None:
+            scale = pick(size, 18, 21, 24)
+            graph, _ = rmat(scale, 16, seed=24, symmetrize=True)
+            name = f"rmat{scale}-sym"
+        self.graphs.append({"name": name, "host": graph, "symmetric": True, "src": 0})
         self.iters = {}
+
+    def check(self, gpu_out, gi):
+        import oracle
+
+        want, it64 = oracle.pr_pull_topo_f64(self.graphs[gi]["host"], 0.85, 1e-6, 1000)
+        err = float(np.abs(gpu_out.view(np.float32).astype(np.float64) - want).max())
+        ok = err <= 1e-5 and abs(self.iters.get(gi, -99) - it64) <= 2
+        return (f"{'within' if ok else 'OUTSIDE'} tolerance: L-inf {err:.2e} vs the FP64 Jacobi oracle (<= 1e-5), "
+                f"{self.iters.get(gi)} iterations vs {it64} (within 2)")
 
     def out_kind(self):
         return ("float32", np.float32)
@@ -541,6 +588,13 @@ class PrResidualJob(PrJob):
     def parity(self, gpu_out, cpu_out, gi):
         err = float(np.abs(gpu_out.view(np.float32).astype(np.float64) - cpu_out).max())
         return f"max abs diff vs CPU fp32 restatement {err:.2e}"
+
+    def check(self, gpu_out, gi):
+        import oracle
+
+        want, _ = oracle.pr_pull_residual(self.graphs[gi]["host"], 0.85, self.tol, 1000, f64=True)
+        err = float(np.abs(gpu_out.view(np.float32).astype(np.float64) - want).max())
+        return f"L-inf {err:.2e} vs the FP64 restatement at the same tolerance"
 
 
 JOBS = {"sssp": SsspJob, "bfs": BfsJob, "bfs-parent": BfsParentJob, "cc": CcJob, "pr": PrJob, "pr-residual": PrResidualJob}
@@ -785,6 +839,121 @@ def run_bc_sharded(args) -> None:
     dist.close()
 
 
+def measure_resident(job: Job, dev: int, dist: Dist, steps: int, warmup: int, order: int) -> dict:
+    """Upload (and reorder) the job's graphs, collect per-call statistics,
+    then time `steps` steps with inputs resident in HBM: CUDA events on the
+    launching stream, barrier + synchronize on both sides, max over ranks."""
+    import torch
+
+    from galois_b200 import DeviceGraph
+
+    tname, _ = job.out_kind()
+    dgs, outs, reorder_ms = [], [], []
+    for g in job.graphs:
+        dg = DeviceGraph(g["host"], symmetric=g["symmetric"], device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if order:
+            dg.reorder(order)  # graph preparation, once, outside the timed region
+        torch.cuda.synchronize()
+        reorder_ms.append((time.perf_counter() - t0) * 1e3)
+        dgs.append(dg)
+        outs.append(torch.empty(g["host"].n, dtype=getattr(torch, tname), device=f"cuda:{dev}"))
+    # stats runs: warm the workspaces, collect units, bytes and kernel time
+    st_runs = [[job.stats_call(dg, gi, outs[gi]) for gi, dg in enumerate(dgs)] for _ in range(3)]
+    stats = st_runs[-1]
+    # the first call of a kernel also pays its lazy module load: average the later runs
+    kms = [sum(r[gi]["kernel_ms"] for r in st_runs[1:]) / (len(st_runs) - 1) for gi in range(len(dgs))]
+    for _ in range(warmup):
+        for gi, dg in enumerate(dgs):
+            job.device_call(dg, gi, outs[gi])
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        for gi, dg in enumerate(dgs):
+            job.device_call(dg, gi, outs[gi])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    t_ms = dist.max(e0.elapsed_time(e1))
+    return {"dgs": dgs, "outs": outs, "stats": stats, "kms": kms, "t_ms": t_ms, "clocks": clk,
+            "reorder_ms": reorder_ms,
+            "units_step": sum(job.units(st, gi) for gi, st in enumerate(stats)),
+            "bytes_step": sum(job.algo_bytes(st, gi) for gi, st in enumerate(stats)),
+            "work_step": sum(job.work_bytes(st, gi) for gi, st in enumerate(stats))}
+
+
+def roofline_of(job: Job, r: dict, order: int, traffic) -> dict:
+    """Roofline of the dominant kernel from its event-timed duration.  `frac`
+    counts the bytes the kernel both had to read and did read: the smaller of
+    the algorithmic model (every reached arc once) and the arcs it actually
+    scanned (direction-optimised BFS and CC's giant skip read fewer arcs than
+    the model, label-correcting SSSP more); both are kept beside it."""
+    peak, peak_src = measured_peak_hbm()
+    sec = sum(r["kms"]) / 1e3
+    need = min(r["bytes_step"], r["work_step"])
+    return {"bound": "hbm", "achieved": need / sec / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": need / sec / 1e9 / peak, "peak_source": peak_src,
+            # a degree-ordered PageRank runs the flat pull kernel
+            "kernel": "pr_pull_flat" if (type(job) is PrJob and order) else job.kernel,
+            "bytes_counted_per_step": need,
+            "algorithmic_bytes_per_step": r["bytes_step"], "kernel_ms_per_step": sum(r["kms"]),
+            "model_frac": r["bytes_step"] / sec / 1e9 / peak,
+            "work_bytes_per_step": r["work_step"],
+            "frac_of_work": r["work_step"] / sec / 1e9 / peak,
+            "traffic": traffic}
+
+
+def run_apps(args, dev: int) -> dict:
+    """The other plain kernels on their configurations, measured in the same
+    run as the headline: BFS on RMAT-20 and RMAT-24, CC and PageRank
+    pull-topological on RMAT-24 (all symmetric ef16, degree-ordered as the
+    headline).  Each entry: device-timed throughput, kernel time, roofline,
+    clocks and parity against the oracle."""
+    import oracle
+    from galois_b200 import rmat
+
+    single = Dist(want_pg=False)
+    g24, _ = rmat(24, 16, seed=24, symmetrize=True)
+    jobs = [("bfs-rmat20", BfsJob("full")),
+            ("bfs-rmat24", BfsJob("full", graph=g24, name="rmat24-sym")),
+            ("cc-rmat24", CcJob("full", graph=g24, name="rmat24-sym")),
+            ("pr-rmat24", PrJob("full", graph=g24, name="rmat24-sym"))]
+    out = {}
+    for key, job in jobs:
+        r = measure_resident(job, dev, single, args.steps, args.warmup, args.order)
+        gpu_host = r["outs"][0].cpu().numpy()
+        for dg in r["dgs"]:
+            dg.free()
+        st = r["stats"][0]
+        # the CPU restatement on the same graph: PageRank counts its own
+        # iterations, the others traverse the same arcs as the GPU
+        t0 = time.perf_counter()
+        if hasattr(job, "cpu_run"):
+            cpu_units = job.cpu_run(job.graphs[0]["host"])[1]
+        else:
+            job.cpu_call(0)
+            cpu_units = r["units_step"]
+        t_cpu = time.perf_counter() - t0
+        out[key] = {"workload": job.workload, "graph": job.graphs[0]["name"], "n": job.graphs[0]["host"].n,
+                    "m": job.graphs[0]["host"].m, "metric": job.metric,
+                    "value": r["units_step"] * args.steps / (r["t_ms"] / 1e3) / 1e9, "unit": job.unit,
+                    "ms_per_step": r["t_ms"] / args.steps, "kernel_ms": sum(r["kms"]),
+                    "roofline": roofline_of(job, r, args.order, None), "clocks": r["clocks"],
+                    "parity": job.check(gpu_host, 0),
+                    "stats": {k: st[k] for k in ("vertices_reached", "edges_reached", "edges_scanned", "rounds",
+                                                 "pull_rounds", "iterations") if k in st},
+                    "cpu_baseline": {"value": cpu_units / t_cpu / 1e9, "unit": job.unit, "cores": oracle.threads(),
+                                     "kind": "port", "sample": "one full run of the same workload"}}
+    return out
+
+
 def cpu_units(job: Job, gpu_stats: list) -> float:
     return sum(job.units(st, gi) for gi, st in enumerate(gpu_stats))
 
@@ -860,78 +1029,33 @@ def main() -> None:
     dev = dist.local_rank
     torch.cuda.set_device(dev)
     job = job_cls(args.size)
-    tname, npdt = job.out_kind()
-    dgs, outs, reorder_ms = [], [], []
-    for g in job.graphs:
-        dg = DeviceGraph(g["host"], symmetric=g["symmetric"], device=dev)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        if args.order:
-            dg.reorder(args.order)  # graph preparation, once, outside the timed region
-        reorder_ms.append((time.perf_counter() - t0) * 1e3)
-        dgs.append(dg)
-        outs.append(torch.empty(g["host"].n, dtype=getattr(torch, tname), device=f"cuda:{dev}"))
-    # stats runs: warm the workspaces, collect units, bytes and kernel time
-    st_runs = [[job.stats_call(dg, gi, outs[gi]) for gi, dg in enumerate(dgs)] for _ in range(3)]
-    stats = st_runs[-1]
-    units_step = sum(job.units(st, gi) for gi, st in enumerate(stats))
-    bytes_step = sum(job.algo_bytes(st, gi) for gi, st in enumerate(stats))
-    work_step = sum(job.work_bytes(st, gi) for gi, st in enumerate(stats))
-    # the first call of a kernel also pays its lazy module load: average the later runs
-    kms = [sum(r[gi]["kernel_ms"] for r in st_runs[1:]) / (len(st_runs) - 1) for gi in range(len(dgs))]
-    for _ in range(args.warmup):
-        for gi, dg in enumerate(dgs):
-            job.device_call(dg, gi, outs[gi])
-    stream = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clocks = ClockSampler(dev)
-    clocks.start()
-    dist.barrier()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        for gi, dg in enumerate(dgs):
-            job.device_call(dg, gi, outs[gi])
-    e1.record(stream)
-    torch.cuda.synchronize()
-    dist.barrier()
-    clk = clocks.stop()
-    t_ms = dist.max(e0.elapsed_time(e1))
+    _, npdt = job.out_kind()
+    r = measure_resident(job, dev, dist, args.steps, args.warmup, args.order)
+    dgs, outs, stats, t_ms = r["dgs"], r["outs"], r["stats"], r["t_ms"]
+    units_step = r["units_step"]
     value = aggregate_rate(dist.world, units_step, args.steps, t_ms)
-    peak, peak_src = measured_peak_hbm()
-    achieved = bytes_step / (sum(kms) / 1e3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_src,
-                # a degree-ordered PageRank runs the flat pull kernel
-                "kernel": "pr_pull_flat" if (type(job) is PrJob and args.order) else job.kernel,
-                "algorithmic_bytes_per_step": bytes_step, "kernel_ms_per_step": sum(kms),
-                # the same over the arcs the kernel actually read
-                "work_bytes_per_step": work_step,
-                "frac_of_work": work_step / (sum(kms) / 1e3) / 1e9 / peak,
-                "traffic": traffic_from_profiles(f"{args.app}-{args.size}")}
+    roofline = roofline_of(job, r, args.order, traffic_from_profiles(f"{args.app}-{args.size}"))
     line = {"metric": job.metric, "value": value, "unit": job.unit, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": job.dtype, "data": "synthetic (seeded generators)",
-            "config": {**job.config(), "vertex_order": ORDER_NAMES[args.order]}, "roofline": roofline, "clocks": clk,
+            "config": {**job.config(), "vertex_order": ORDER_NAMES[args.order]}, "roofline": roofline,
+            "clocks": r["clocks"],
             "gpu_launches": sum(int(st["launches"]) for st in stats) * args.steps,
-            "reorder_ms": reorder_ms,
+            "reorder_ms": r["reorder_ms"],
             "detail": [{"graph": job.graphs[gi]["name"], **{k: stats[gi][k] for k in stats[gi]}}
                        for gi in range(len(dgs))]}
     # ---- CPU baseline (rank 0, one GPU only) -----------------------------------
     if dist.world == 1 and not args.no_cpu_baseline:
         import oracle
 
-        if isinstance(job, (CcJob, PrJob)) and args.size == "full":
-            # bounded sample: the same algorithm on RMAT-22 sym (a full RMAT-24
-            # run of the CPU restatement takes minutes)
-            from galois_b200 import rmat
-
-            gs, _ = rmat(22, 16, seed=24, symmetrize=True)
+        if isinstance(job, (CcJob, PrJob)):
+            # the same algorithm on the same graph; PageRank's units count the
+            # CPU restatement's own iterations
             t0 = time.perf_counter()
-            _, cu = job.cpu_run(gs)
+            _, cu = job.cpu_run(job.graphs[0]["host"])
             t_cpu = time.perf_counter() - t0
             line["cpu_baseline"] = {"value": cu / t_cpu / 1e9, "unit": job.unit, "cores": oracle.threads(),
-                                    "kind": "port", "sample": "same algorithm on RMAT-22 sym ef16 (bounded sample)"}
+                                    "kind": "port", "sample": "one full run of the workload's graph"}
         else:
             t0 = time.perf_counter()
             cpu_outs = [job.cpu_call(gi) for gi in range(len(job.graphs))]
@@ -940,6 +1064,7 @@ def main() -> None:
             line["cpu_baseline"] = {"value": units_step / t_cpu / 1e9, "unit": job.unit,
                                     "cores": 1 if getattr(job, "cpu_serial", False) else oracle.threads(),
                                     "kind": "port", "sample": "one full run of every graph of the workload",
+                                    **({"schedule": SsspJob.CPU_SCHEDULE} if isinstance(job, SsspJob) else {}),
                                     "parity": [job.parity(gpu_host[gi], cpu_outs[gi], gi)
                                                for gi in range(len(job.graphs))]}
     # ---- end to end through the public API with host buffers -----------------
@@ -979,6 +1104,9 @@ def main() -> None:
                                "amortise gb_graph_reorder) + kernel + host output copy + gb_graph_free"}
     for dg in dgs:
         dg.free()
+    # ---- the other plain kernels on their configurations (one GPU) ------------
+    if args.app == "sssp" and args.size == "full" and dist.world == 1 and not args.no_apps:
+        line["apps"] = run_apps(args, dev)
     if dist.rank == 0:
         emit(line)
     dist.close()

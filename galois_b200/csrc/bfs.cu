@@ -492,11 +492,11 @@ extern "C" int gb_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* 
 // bitmaps and levels are rewritten by the init kernel).  Calls that overlap
 // on the GPU (other streams, other host threads) race on the array and must
 // be serialised by the caller.
-// The first call on a device looks up the array's device address with
-// cudaGetSymbolAddress (with that device current); make that first call
-// before any stream capture on the device.
+// Every call looks up the array's device address on the current device with
+// cudaGetSymbolAddress (cheap), so no address is kept across calls, devices or
+// a cudaDeviceReset.  The call is synchronous: it waits for `stream` to finish
+// the validation and the BFS before it returns.
 // ---------------------------------------------------------------------------
-#include <mutex>
 
 namespace gb {
 namespace {
@@ -518,24 +518,30 @@ constexpr size_t kNoAllocScratchBytes =
 
 static __device__ __align__(256) unsigned char g_bfs_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-void* g_noalloc_addr[kMaxDevices] = {};
-std::mutex g_noalloc_mu;
-
-// Device address of the scratch array for the current device (looked up once
-// per device; host code must never pass the symbol itself to a kernel).
+// Device address of the scratch array on the current device.  Host code sees
+// only a host-side stand-in under the array's name, never the device address,
+// so the symbol itself must never be passed to a kernel.
 int noalloc_scratch(void** out) {
-  int dev = 0;
-  GB_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) GB_FAIL(GB_ERR_UNSUPPORTED, "gb_bfs_noalloc: device %d out of range", dev);
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_bfs_noalloc_scratch);
-    if (e != cudaSuccess || !p) return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
-    g_noalloc_addr[dev] = p;
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_bfs_noalloc_scratch);
+  if (e != cudaSuccess || !p) return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
+  *out = p;
+  return GB_OK;
+}
+
+// GB_OK if p is device (or managed) memory that the current device `dev` can
+// address as its own; a pointer into another GPU's memory would make the
+// kernels fault instead of returning an error.
+int noalloc_check_ptr(const void* p, const char* what, int dev) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    GB_FAIL(GB_ERR_ARG, "gb_bfs_noalloc: %s is not device memory", what);
   }
-  *out = g_noalloc_addr[dev];
+  if (at.type == cudaMemoryTypeManaged) return GB_OK;
+  if (at.type != cudaMemoryTypeDevice) GB_FAIL(GB_ERR_ARG, "gb_bfs_noalloc: %s is not device memory", what);
+  if (at.device != dev)
+    GB_FAIL(GB_ERR_ARG, "gb_bfs_noalloc: %s lives on device %d, the current device is %d", what, at.device, dev);
   return GB_OK;
 }
 
@@ -564,10 +570,14 @@ extern "C" int gb_bfs_noalloc(const uint64_t* offs, const uint32_t* col, uint32_
     GB_FAIL(GB_ERR_CAPACITY, "gb_bfs_noalloc: graph of %u vertices / %llu arcs exceeds the fixed scratch "
             "(at most %u vertices and %llu arcs); use gb_bfs", n, (unsigned long long)m, kNoAllocMaxNodes,
             (unsigned long long)kNoAllocMaxArcs);
-  if (!is_device_ptr(offs) || !is_device_ptr(col) || !is_device_ptr(level_out))
-    GB_FAIL(GB_ERR_ARG, "gb_bfs_noalloc: offs, col and level_out must be device memory");
+  int dev = 0, sms = 0;
+  GB_CUDA(cudaGetDevice(&dev));
+  int st = noalloc_check_ptr(offs, "offs", dev);
+  if (st == GB_OK) st = noalloc_check_ptr(col, "col", dev);
+  if (st == GB_OK) st = noalloc_check_ptr(level_out, "level_out", dev);
+  if (st != GB_OK) return st;
   void* base = nullptr;
-  int st = noalloc_scratch(&base);
+  st = noalloc_scratch(&base);
   if (st != GB_OK) return st;
   const uint32_t words = (n + 31) / 32;
   const FrontierLayout fl = frontier_layout(n, m, kNoAllocHeavy, kNoAllocTile);
@@ -596,8 +606,6 @@ extern "C" int gb_bfs_noalloc(const uint64_t* offs, const uint32_t* col, uint32_
   a.alpha = 15.f;
   a.beta = 18.f;
   a.max_levels = n + 1;
-  int dev = 0, sms = 0;
-  GB_CUDA(cudaGetDevice(&dev));
   GB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   // the array keeps the previous call's contents: clear the control block and
   // the validation flag (bitmaps and levels are rewritten by bfs_init)

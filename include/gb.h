@@ -246,8 +246,13 @@ int gb_bfs_parent(gb_graph* g, uint32_t src, uint32_t* parent_out,
  * ids, level_out: n) with all scratch in a fixed file-scope device array that
  * every GPU loading libgb keeps until exit.  Limits: n <= 2^20, m <= 2^26
  * (GB_ERR_CAPACITY beyond).  Calls share the array: calls that overlap on the
- * GPU race.  The first call on a device looks up the array's address; make it
- * before any stream capture.  symmetric != 0 allows bottom-up steps. */
+ * GPU race.  The three arrays must live on the current device (GB_ERR_ARG
+ * otherwise); an invalid CSR (offsets not monotone or not ending at m, an id
+ * >= n) returns GB_ERR_FORMAT before level_out is written.  The call is
+ * synchronous (it waits for `stream`).  symmetric != 0 declares that every
+ * arc (u,v) has its reverse (v,u), as gb_graph_upload's flag does, and lets
+ * bottom-up steps read the out-arcs as in-arcs; a directed graph must pass 0
+ * (push-only levels), or its levels come out wrong. */
 int gb_bfs_noalloc(const uint64_t* offs, const uint32_t* col, uint32_t n,
                    uint64_t m, int symmetric, uint32_t src,
                    uint32_t* level_out, void* stream);

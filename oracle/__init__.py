@@ -68,6 +68,8 @@ _SIG = {
     "orc_bc_level": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
     "orc_bc_level_f64": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
     "orc_bc_level_par": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
+    "orc_bc_level_f64_par_sources": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
+    "orc_ppr_solve_f64": (_u32, [_u32, _vp, _vp, _vp, _vp, C.c_double, C.c_double, _u32, C.c_int, _vp]),
 }
 for _n, (_r, _a) in _SIG.items():
     _f = getattr(_lib, _n)
@@ -296,9 +298,15 @@ def pr_push_sync(g, alpha=0.85, tol=1e-3, max_iter=1000, f64=True) -> tuple[np.n
 
 
 def bc_level(g, sources, f64: bool = False, parallel: bool = False) -> np.ndarray:
+    """Level BC summed over `sources`.  f64: FP64 sigma, dependency and bc
+    (parallel: sources spread over the threads); else the reference's types
+    (fp64 sigma, fp32 dependency; parallel: all threads on one source)."""
     n, end, col = _g(g)
     src = np.ascontiguousarray(np.asarray(sources, np.uint32))
-    if f64:
+    if f64 and parallel:
+        out = np.empty(n, np.float64)
+        _lib.orc_bc_level_f64_par_sources(n, _p(end), _p(col), _p(src), src.size, _p(out))
+    elif f64:
         out = np.empty(n, np.float64)
         _lib.orc_bc_level_f64(n, _p(end), _p(col), _p(src), src.size, _p(out))
     else:
@@ -306,3 +314,16 @@ def bc_level(g, sources, f64: bool = False, parallel: bool = False) -> np.ndarra
         fn = _lib.orc_bc_level_par if parallel else _lib.orc_bc_level
         fn(n, _p(end), _p(col), _p(src), src.size, _p(out))
     return out
+
+
+def ppr_solve_f64(g, w, rhs, alpha=0.85, tol=1e-13, max_iter=10000, adjoint=False) -> tuple[np.ndarray, int]:
+    """FP64 Jacobi solve of one PPR column: x = rhs + alpha W~ x, or with
+    adjoint the transposed system lam = rhs + alpha W~^T lam (the conventions
+    of oracle/ppr.py), stopped at an L1 change <= tol * max(1, |rhs|_1)."""
+    n, end, col = _g(g)
+    wf = np.ascontiguousarray(w, np.float32)
+    r = np.ascontiguousarray(rhs, np.float64)
+    out = np.empty(n, np.float64)
+    it = _lib.orc_ppr_solve_f64(n, _p(end), _p(col), _p(wf), _p(r), alpha, tol, max_iter, 1 if adjoint else 0,
+                                _p(out))
+    return out, int(it)

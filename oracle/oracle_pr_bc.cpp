@@ -354,4 +354,87 @@ void orc_bc_level_par(uint32_t n, const uint64_t* end, const uint32_t* col, cons
   }
 }
 
+// Level BC in FP64 with the sources spread over the threads (each thread runs
+// whole sources with its own arrays and the per-thread sums are added at the
+// end): the FP64 ground truth for batches of many sources on large graphs.
+void orc_bc_level_f64_par_sources(uint32_t n, const uint64_t* end, const uint32_t* col, const uint32_t* srcs,
+                                  uint32_t nsrc, double* bc) {
+  Csr g{n, end, col};
+  for (uint32_t v = 0; v < n; ++v) bc[v] = 0;
+#pragma omp parallel
+  {
+    std::vector<double> mine(n, 0.0), one(n);
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t s = 0; s < (int64_t)nsrc; ++s) {
+      bc_level<double, double, double>(g, srcs + s, 1, one.data());
+      for (uint32_t v = 0; v < n; ++v) mine[v] += one[v];
+    }
+#pragma omp critical
+    for (uint32_t v = 0; v < n; ++v) bc[v] += mine[v];
+  }
+}
+
+// FP64 Jacobi solve of one personalised-PageRank column (no reference: the
+// PPR addition's ground truth on graphs too large for a sparse LU).  Arcs
+// j->i in CSR order with weight w[e]; s_j = out-weight sum of j;
+// W~_ij = w_ji / s_j.  adjoint == 0: x = rhs + alpha W~ x (rhs = (1-alpha) T);
+// adjoint != 0: lam = rhs + alpha W~^T lam (rhs = dL/dx).  Iterates from
+// out = rhs until the L1 change is <= tol * max(1, |rhs|_1) or max_iter;
+// returns the iteration count.
+uint32_t orc_ppr_solve_f64(uint32_t n, const uint64_t* end, const uint32_t* col, const float* w, const double* rhs,
+                           double alpha, double tol, uint32_t max_iter, int adjoint, double* out) {
+  Csr g{n, end, col};
+  std::vector<double> s(n, 0.0);
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int64_t j = 0; j < (int64_t)n; ++j) {
+    double t = 0;
+    for (uint64_t e = g.b((uint32_t)j); e < g.e((uint32_t)j); ++e) t += w[e];
+    s[j] = t;
+  }
+  // in-arcs (forward pulls x_j over arcs j->i): counting sort by target
+  std::vector<uint64_t> tb;
+  std::vector<uint32_t> tsrc;
+  std::vector<double> tcoef;
+  const uint64_t m = n ? end[n - 1] : 0;
+  if (!adjoint) {
+    tb.assign((size_t)n + 1, 0);
+    for (uint64_t e = 0; e < m; ++e) tb[col[e] + 1]++;
+    for (uint32_t i = 0; i < n; ++i) tb[i + 1] += tb[i];
+    std::vector<uint64_t> fill(tb.begin(), tb.end() - 1);
+    tsrc.resize(m);
+    tcoef.resize(m);
+    for (uint32_t j = 0; j < n; ++j)
+      for (uint64_t e = g.b(j); e < g.e(j); ++e) {
+        const uint64_t k = fill[col[e]]++;
+        tsrc[k] = j;
+        tcoef[k] = s[j] > 0 ? (double)w[e] / s[j] : 0.0;
+      }
+  }
+  double rn = 0;
+  for (uint32_t v = 0; v < n; ++v) rn += std::fabs(rhs[v]);
+  const double stop = tol * (rn > 1.0 ? rn : 1.0);
+  std::vector<double> nx(n);
+  for (uint32_t v = 0; v < n; ++v) out[v] = rhs[v];
+  uint32_t it = 0;
+  while (it < max_iter) {
+    double l1 = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : l1)
+    for (int64_t v = 0; v < (int64_t)n; ++v) {
+      double acc = 0;
+      if (adjoint) {
+        for (uint64_t e = g.b((uint32_t)v); e < g.e((uint32_t)v); ++e)
+          acc += (s[v] > 0 ? (double)w[e] / s[v] : 0.0) * out[col[e]];
+      } else {
+        for (uint64_t k = tb[v]; k < tb[v + 1]; ++k) acc += tcoef[k] * out[tsrc[k]];
+      }
+      nx[v] = rhs[v] + alpha * acc;
+      l1 += std::fabs(nx[v] - out[v]);
+    }
+    for (uint32_t v = 0; v < n; ++v) out[v] = nx[v];
+    ++it;
+    if (l1 <= stop) break;
+  }
+  return it;
+}
+
 }  // extern "C"

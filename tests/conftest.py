@@ -1,4 +1,3 @@
-import os
 import sys
 from pathlib import Path
 
@@ -24,5 +23,3 @@ def cuda_device():
     torch.cuda.init()
     return 0
 
-
-REFERENCE = Path(os.environ.get("GALOIS_REFERENCE", "/root/reference"))

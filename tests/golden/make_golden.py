@@ -9,19 +9,23 @@
    sizes, so that a change to the generators (which would silently change every
    benchmark input) fails a test.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:
+    python tests/golden/make_golden.py [--reference PATH_TO_GALOIS_TREE]
+(or set GALOIS_REFERENCE).  Without a reference tree the graph_convert/
+fixtures already committed are kept and only generators.json is rewritten.
 """
 from __future__ import annotations
 
+import argparse
 import hashlib
 import json
+import os
 import shutil
 import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF = Path("/root/reference/tools/graph-convert/test-inputs")
 
 
 def digest(*arrays) -> str:
@@ -33,9 +37,14 @@ def digest(*arrays) -> str:
 
 
 def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("GALOIS_REFERENCE"),
+                    help="root of a Galois source tree (its tools/graph-convert/test-inputs are copied)")
+    args = ap.parse_args()
     out = HERE / "graph_convert"
     out.mkdir(exist_ok=True)
-    if REF.exists():
+    REF = Path(args.reference) / "tools" / "graph-convert" / "test-inputs" if args.reference else None
+    if REF is not None and REF.exists():
         for f in sorted(REF.iterdir()):
             shutil.copyfile(f, out / f.name)
     sys.path.insert(0, str(ROOT))

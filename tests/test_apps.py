@@ -163,7 +163,8 @@ def test_bc_gpu_app(cuda_device, graphs, tmp_path):
         parts = ln.split()
         if len(parts) == 2 and parts[0].isdigit():
             got[int(parts[0])] = float(parts[1])
-    assert np.max(np.abs(got - want)) <= 1e-4 * max(1.0, float(np.max(want)))
+    # per vertex, relative to max(|fp64|, 1): the -output lines carry 9 decimals
+    assert np.max(np.abs(got - want) / np.maximum(np.abs(want), 1.0)) <= 1e-6
 
 
 @pytest.mark.gpu

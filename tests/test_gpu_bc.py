@@ -1,7 +1,7 @@
 """GPU parity for Brandes BC (single-source looped and multi-source batched)
 against the CPU restatement of LevelStructs.h in FP64.
 
-Tolerance: |gpu - fp64| <= 1e-5 * max(|fp64|, 1) per vertex.  The GPU keeps
+Tolerance: |gpu - fp64| <= 1e-6 * max(|fp64|, 1) per vertex.  The GPU keeps
 sigma in fp64 and accumulates bc in fp64 but stores dependencies in fp32 as the
 reference does, so each source contributes ~1e-7 relative rounding."""
 import numpy as np
@@ -20,7 +20,7 @@ def path_graph(n):
     return HostCSR.from_edges(n, s, d)
 
 
-def close(got, want, rtol=1e-5):
+def close(got, want):
     scale = np.maximum(np.abs(want), 1.0)
     return float((np.abs(got.astype(np.float64) - want) / scale).max())
 
@@ -33,7 +33,7 @@ def test_bc_rmat_matches_fp64(cuda_device, batch):
     want = oracle.bc_level(g, srcs, f64=True)
     with DeviceGraph(g, symmetric=True) as dg:
         got = dg.bc(srcs, batch=batch)
-    assert close(got, want) < 1e-5
+    assert close(got, want) < 1e-6
 
 
 def test_bc_heavy_tiles_and_duplicates(cuda_device):
@@ -45,7 +45,7 @@ def test_bc_heavy_tiles_and_duplicates(cuda_device):
     with DeviceGraph(g, symmetric=True) as dg:
         dg.set_tuning(heavy_degree=16, tile_edges=32)
         for batch in (1, 5):
-            assert close(dg.bc(srcs, batch=batch), want) < 1e-5
+            assert close(dg.bc(srcs, batch=batch), want) < 1e-6
 
 
 def test_bc_path_closed_form(cuda_device):
@@ -62,7 +62,7 @@ def test_bc_directed_single_source_and_errors(cuda_device):
     srcs = np.array([perm[0], perm[1], perm[2]], np.uint32)
     want = oracle.bc_level(g, srcs, f64=True)
     with DeviceGraph(g, symmetric=False) as dg:
-        assert close(dg.bc(srcs, batch=1), want) < 1e-5
+        assert close(dg.bc(srcs, batch=1), want) < 1e-6
         with pytest.raises(GbError) as e:
             dg.bc(srcs, batch=3)
         assert e.value.status == _lib.GB_ERR_UNSUPPORTED
