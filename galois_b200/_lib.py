@@ -65,7 +65,8 @@ class Stats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("heavy_degree", C.c_uint32), ("tile_edges", C.c_uint32), ("block_threads", C.c_uint32),
                 ("blocks_per_sm", C.c_uint32), ("do_alpha", C.c_float), ("do_beta", C.c_float),
-                ("direction_opt", C.c_int), ("local_depth", C.c_int)]
+                ("direction_opt", C.c_int), ("local_depth", C.c_int),
+                ("sssp_async", C.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -103,6 +104,7 @@ SIGNATURES: dict[str, tuple] = {
     "gb_gen_er": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, _csrp]),
     "gb_assign_weights_u32": (C.c_int, [_csrp, C.c_uint32, C.c_uint32, C.c_uint64]),
     "gb_assign_weights_f32": (C.c_int, [_csrp, C.c_uint64]),
+    "gb_assign_weights_reference": (C.c_int, [_csrp, C.c_int, C.c_int, C.c_int]),
     "gb_transpose_host": (C.c_int, [_csrp, _csrp, _u64p]),
     "gb_graph_upload": (C.c_int, [_vp, _vp, _vp, _vp, C.c_uint32, C.c_uint64, C.c_int, C.c_int,
                                   C.POINTER(_gp)]),
@@ -115,6 +117,7 @@ SIGNATURES: dict[str, tuple] = {
     "gb_graph_symmetrize": (C.c_int, [_gp, C.c_int, _vp]),
     "gb_graph_assign_weights_u32": (C.c_int, [_gp, C.c_uint32, C.c_uint32, C.c_uint64, _vp]),
     "gb_graph_assign_weights_f32": (C.c_int, [_gp, C.c_uint64, _vp]),
+    "gb_graph_assign_weights_reference": (C.c_int, [_gp, C.c_int, C.c_int, C.c_int, _vp]),
     "gb_graph_reorder": (C.c_int, [_gp, C.c_int, _vp]),
     "gb_pool_trim": (C.c_int, []),
     "gb_graph_permutation": (C.c_int, [_gp, C.POINTER(_vp), C.POINTER(_vp)]),

@@ -42,9 +42,10 @@ std::string tuning_json(const gb_tuning& t) {
   char buf[256];
   std::snprintf(buf, sizeof(buf),
                 "{\"heavy_degree\": %u, \"tile_edges\": %u, \"block_threads\": %u, \"blocks_per_sm\": %u, "
-                "\"do_alpha\": %g, \"do_beta\": %g, \"direction_opt\": %d, \"local_depth\": %d}",
+                "\"do_alpha\": %g, \"do_beta\": %g, \"direction_opt\": %d, \"local_depth\": %d, "
+                "\"sssp_async\": %d}",
                 t.heavy_degree, t.tile_edges, t.block_threads, t.blocks_per_sm, t.do_alpha, t.do_beta,
-                t.direction_opt, t.local_depth);
+                t.direction_opt, t.local_depth, t.sssp_async);
   return buf;
 }
 
@@ -74,6 +75,7 @@ bool cache_lookup(const char* path, const std::string& cls, const std::string& k
     if (parse_field(line, "do_beta", &v)) r.do_beta = (float)v;
     if (parse_field(line, "direction_opt", &v)) r.direction_opt = (int)v;
     if (parse_field(line, "local_depth", &v)) r.local_depth = (int)v;
+    if (parse_field(line, "sssp_async", &v)) r.sssp_async = (int)v;
     *t = r;
     found = true;  // the last matching line wins
   }
@@ -115,7 +117,12 @@ extern "C" int gb_autotune(gb_graph* g, const char* kernel, uint32_t src, const 
       if (k == "sssp") {
         for (int depth : {-1, 2, 8, 16}) {
           t.local_depth = depth;
+          t.sssp_async = -1;
           cands.push_back(t);
+          if (depth > 0) {  // asynchronous buckets (taken only when every vertex is light)
+            t.sssp_async = 0;
+            cands.push_back(t);
+          }
         }
       } else if (k == "bfs") {
         for (float alpha : {5.f, 15.f, 40.f}) {

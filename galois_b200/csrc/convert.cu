@@ -22,6 +22,8 @@
 //    counter-based stream (the host generators' stream_key / rand_at), so the
 //    device fills every arc in parallel and matches gb_assign_weights_u32 /
 //    _f32 on the host bit for bit.
+//  * gb_graph_assign_weights_reference: the reference converter's own draws
+//    (one sequential std::mt19937 stream), made on the host and uploaded.
 
 #include <algorithm>
 
@@ -281,6 +283,34 @@ int gb_graph_assign_weights_f32(gb_graph* g, uint64_t seed, void* stream) {
   }
   if (g->m) weights_f32_kernel<<<grid_for(g, g->m), 256, 0, s>>>(g->wf, g->m, stream_key(seed, kTagWeightF32));
   GB_CUDA(cudaGetLastError());
+  return GB_OK;
+}
+
+int gb_graph_assign_weights_reference(gb_graph* g, int min_value, int max_value, int edge_bytes, void* stream) {
+  using namespace gb;
+  clear_error();
+  if (!g) GB_FAIL(GB_ERR_ARG, "gb_graph_assign_weights_reference: null graph");
+  int st = check_reference_weights(min_value, max_value, edge_bytes, "gb_graph_assign_weights_reference");
+  if (st != GB_OK) return st;
+  if (g->perm)
+    GB_FAIL(GB_ERR_UNSUPPORTED, "gb_graph_assign_weights_reference: assign weights before gb_graph_reorder");
+  GB_CUDA(cudaSetDevice(g->device));
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (edge_bytes == -4) drop_derived(g);  // float weights feed the transpose's copy and the PPR state
+  void** dst = edge_bytes == 4 ? reinterpret_cast<void**>(&g->w) : reinterpret_cast<void**>(&g->wf);
+  const size_t bytes = 4 * std::max<uint64_t>(g->m, 1);
+  if (!*dst) {
+    cudaError_t e = pool_malloc(dst, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "gb_graph_assign_weights_reference");
+  }
+  void* h = nullptr;
+  cudaError_t e = pool_malloc_host(&h, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "gb_graph_assign_weights_reference");
+  draw_reference_weights(g->m, min_value, max_value, edge_bytes, h);
+  e = cudaMemcpyAsync(*dst, h, 4 * g->m, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  pool_free_host(h);
+  if (e != cudaSuccess) return cuda_fail(e, "gb_graph_assign_weights_reference");
   return GB_OK;
 }
 

@@ -45,6 +45,12 @@ enum : uint64_t {
   kTagEr = 5,
 };
 
+// gr2randomweightgr's weights (host_graph.cpp): argument check, then the
+// draws of a default std::mt19937 in arc order into out[m] (uint32 for
+// edge_bytes 4, float for -4).
+int check_reference_weights(int min_value, int max_value, int edge_bytes, const char* what);
+void draw_reference_weights(uint64_t m, int min_value, int max_value, int edge_bytes, void* out);
+
 }  // namespace gb
 
 #define GB_FAIL(code, ...)        \

@@ -17,6 +17,7 @@
 #include <cerrno>
 #include <cmath>
 #include <cstdlib>
+#include <random>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -125,6 +126,37 @@ int build_csr_from_stream(uint32_t n, uint64_t ndraws, Emit emit,
 }  // namespace gb
 
 using namespace gb;
+
+namespace gb {
+
+int check_reference_weights(int min_value, int max_value, int edge_bytes, const char* what) {
+  if (edge_bytes != 4 && edge_bytes != -4) GB_FAIL(GB_ERR_ARG, "%s: edge_bytes must be 4 (uint32) or -4 (float)", what);
+  if (max_value < min_value) GB_FAIL(GB_ERR_ARG, "%s: max_value < min_value", what);
+  if (edge_bytes == 4 && min_value < 0) GB_FAIL(GB_ERR_ARG, "%s: uint32 weights need min_value >= 0", what);
+  return GB_OK;
+}
+
+// gr2randomweightgr's draws (tools/graph-convert/graph-convert.cpp:1145-1190):
+// one default-constructed std::mt19937 and a std::uniform_int_distribution
+// <uint32_t>(min, max) (edge_bytes 4) or std::uniform_real_distribution
+// <float>(min, max) (edge_bytes -4), evaluated once per arc in arc order.
+// The draws come from this build's C++ standard library, so they equal the
+// converter's output when both use the same library (the distributions'
+// algorithms are implementation-defined).
+void draw_reference_weights(uint64_t m, int min_value, int max_value, int edge_bytes, void* out) {
+  std::mt19937 gen;
+  if (edge_bytes == 4) {
+    std::uniform_int_distribution<uint32_t> dist((uint32_t)min_value, (uint32_t)max_value);
+    uint32_t* w = static_cast<uint32_t*>(out);
+    for (uint64_t e = 0; e < m; ++e) w[e] = dist(gen);
+  } else {
+    std::uniform_real_distribution<float> dist((float)min_value, (float)max_value);
+    float* w = static_cast<float*>(out);
+    for (uint64_t e = 0; e < m; ++e) w[e] = dist(gen);
+  }
+}
+
+}  // namespace gb
 
 extern "C" {
 
@@ -487,6 +519,26 @@ int gb_assign_weights_f32(gb_host_csr* g, uint64_t seed) {
     const uint64_t r = (rand_at(key, (uint64_t)e) >> 40) + 1;
     g->w_f32[e] = (float)r * (1.0f / 16777216.0f);
   }
+  return GB_OK;
+}
+
+// gr2randomweightgr exactly as the reference converter draws its weights
+// (tools/graph-convert/graph-convert.cpp:1145-1190): one default-constructed
+// std::mt19937 and a std::uniform_int_distribution<uint32_t>(min, max) (or
+// std::uniform_real_distribution<float>(min, max)) evaluated once per arc in
+// arc order.  The draws come from this build's C++ standard library, so they
+// equal the converter's output when both use the same library (the
+// distributions' algorithms are implementation-defined).
+int gb_assign_weights_reference(gb_host_csr* g, int min_value, int max_value, int edge_bytes) {
+  clear_error();
+  if (!g) GB_FAIL(GB_ERR_ARG, "gb_assign_weights_reference: null graph");
+  const int st = check_reference_weights(min_value, max_value, edge_bytes, "gb_assign_weights_reference");
+  if (st != GB_OK) return st;
+  void** slot = edge_bytes == 4 ? reinterpret_cast<void**>(&g->w_u32) : reinterpret_cast<void**>(&g->w_f32);
+  std::free(*slot);
+  *slot = xmalloc<uint32_t>(g->m);
+  if (!*slot && g->m) GB_FAIL(GB_ERR_OOM, "host allocation failed");
+  draw_reference_weights(g->m, min_value, max_value, edge_bytes, *slot);
   return GB_OK;
 }
 

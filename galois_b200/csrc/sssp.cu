@@ -40,6 +40,19 @@
 // vertices move to the near queue and the rest are compacted.  Phases are
 // separated by the bounded grid barrier.
 
+//
+// Bounded-degree graphs (every vertex light and the local queues on: grids,
+// road-like graphs) run an asynchronous form instead (sssp_async below): the
+// phases of a bucket are not separated by grid barriers at all.  Each warp
+// keeps relaxing its own local queue; improvements that do not fit, and a
+// warp's surplus while other warps wait for work, are published as chunks of
+// up to 32 entries in a ring; a warp without work takes the next ring
+// position (a ticket) and waits for its chunk.  A bucket ends when a single
+// counter -- busy warps plus published, unconsumed chunks -- reaches zero;
+// only the bucket transitions keep grid barriers.  On such graphs a bucket's
+// shortest-path chains are hundreds of hops long and the phase barrier, not
+// the relaxations, set the time.
+
 #include "device_common.cuh"
 #include "device_graph.cuh"
 #include "frontier.cuh"
@@ -75,6 +88,30 @@ struct SsspCtl {
   unsigned long long relax;
 };
 
+// Control words of the chunk ring of sssp_async, each on its own 128-byte line
+// (every waiting warp polls them).
+struct alignas(128) RingCtl {
+  unsigned long long head;  // ring positions taken by warps waiting for work (tickets)
+  unsigned long long pad0[15];
+  unsigned long long tail;  // ring positions published
+  unsigned long long pad1[15];
+  int work;  // busy warps + published chunks not yet taken: 0 ends the bucket
+  int pad2[31];
+  unsigned long long chunks;  // chunks published (statistics)
+  unsigned long long pad3[15];
+};
+
+// The chunk ring: position p lives in slot p & mask.  seq[slot] == p: free for
+// the producer of position p; == p + 1: published, for the consumer of p;
+// the consumer sets it to p + cap, freeing the slot for the next lap.
+struct ChunkRing {
+  uint4* ent;               // [cap][32] entries (vertex, dist, begin lo, begin hi << 16 | degree)
+  unsigned long long* seq;  // [cap]
+  uint32_t* cnt;            // [cap] entries in the chunk
+  unsigned long long mask;  // cap - 1 (cap a power of two)
+  RingCtl* rc;
+};
+
 struct SsspArgs {
   const uint64_t* __restrict__ offs;
   const uint32_t* __restrict__ col;
@@ -97,6 +134,7 @@ struct SsspArgs {
   const uint2* sw_tiles;  // cached (vertex, k) tiles of every heavy vertex
   uint32_t sw_ntiles;
   uint32_t bm_min;  // frontier estimate above which the next frontier is a bitmap
+  ChunkRing ring;   // sssp_async only
 };
 
 __global__ void sssp_init(SsspArgs a) {
@@ -496,6 +534,295 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
   if (gtid == 0) ctl->phases = P;
 }
 
+// ---- asynchronous buckets (bounded-degree graphs) ----------------------------
+
+constexpr int kAsyncLQ = 64;                          // local-queue entries per warp
+constexpr uint64_t kRingSlotWaitNs = 2000000000ull;   // a producer's wait for a free slot
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
+  return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+
+// Publish the entries of the lanes with `pred` as one chunk (warp-collective).
+// The chunk is counted in `work` before it becomes visible, while this warp
+// is itself busy, so the count never reads zero with work outstanding.
+// Returns false when the slot stayed occupied past the wait limit (the ring
+// is full; the error word is raised) or another warp raised an error.
+__device__ __forceinline__ bool ring_publish(const ChunkRing& r, bool pred, uint4 e, int* err) {
+  const unsigned m = __ballot_sync(kFull, pred);
+  if (!m) return true;
+  const uint32_t lane = lane_id();
+  unsigned long long p = 0;
+  int ok = 1;
+  if (lane == 0) {
+    atomicAdd(&r.rc->work, 1);
+    p = atomicAdd(&r.rc->tail, 1ull);
+    atomicAdd(&r.rc->chunks, 1ull);
+    // the slot is free once the consumer of the previous lap released it
+    const unsigned long long* sq = r.seq + (p & r.mask);
+    uint64_t t0 = 0;
+    unsigned spins = 0;
+    while (ld_acquire_u64(sq) != p) {
+      if ((++spins & 63u) == 0) {
+        const uint64_t now = globaltimer_ns();
+        if (!t0) t0 = now;
+        if (read_err(err)) { ok = 0; break; }
+        if (now - t0 > kRingSlotWaitNs) { raise_err(err, kDevOverflow); ok = 0; break; }
+      }
+      __nanosleep(64);
+    }
+  }
+  p = __shfl_sync(kFull, p, 0);
+  ok = __shfl_sync(kFull, ok, 0);
+  if (!ok) return false;
+  const unsigned long long slot = p & r.mask;
+  if (pred) r.ent[slot * 32 + __popc(m & ((1u << lane) - 1u))] = e;
+  if (lane == 0) r.cnt[slot] = (uint32_t)__popc(m);
+  __syncwarp();
+  if (lane == 0) {
+    __threadfence();
+    st_release_u64(r.seq + slot, p + 1);
+  }
+  return true;
+}
+
+// Lane 0 of a warp without work: wait for the chunk of ring position p.
+// 1: published; 0: the bucket has no work left anywhere; -1: an error was
+// raised or the kernel passed its deadline (kDevTimeout raised).
+__device__ __forceinline__ int ring_wait(const ChunkRing& r, unsigned long long p, int* err, uint64_t deadline) {
+  const unsigned long long* sq = r.seq + (p & r.mask);
+  unsigned spins = 0, ns = 32;
+  for (;;) {
+    if (ld_acquire_u64(sq) == p + 1) return 1;
+    if ((++spins & 7u) == 0) {
+      // work counts every busy warp and every published chunk, ours included
+      if (*reinterpret_cast<const volatile int*>(&r.rc->work) == 0) return 0;
+      if (read_err(err)) return -1;
+      if (globaltimer_ns() > deadline) {
+        raise_err(err, kDevTimeout);
+        return -1;
+      }
+    }
+    __nanosleep(ns);
+    if (ns < 512) ns <<= 1;
+  }
+}
+
+__global__ void sssp_async_init(SsspArgs a) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t words = (a.n + 31) >> 5;
+  for (uint64_t v = tid; v < a.n; v += stride) a.dist[v] = (v == a.src) ? 0u : kInf;
+  for (uint64_t w = tid; w < words; w += stride) a.infar[w] = 0;
+  const uint64_t b = a.offs[a.src], d = a.offs[a.src + 1] - b;
+  for (uint64_t i = tid; i <= a.ring.mask; i += stride) {
+    if (i == 0 && d > 0) {
+      // the source, published as the chunk of position 0 (counted in work)
+      a.ring.ent[0] = make_uint4(a.src, 0u, (uint32_t)b, (uint32_t)((b >> 32) << 16) | (uint32_t)d);
+      a.ring.cnt[0] = 1;
+      a.ring.seq[0] = 1;
+      a.ring.rc->tail = 1;
+      a.ring.rc->work = 1;
+    } else {
+      a.ring.seq[i] = i;
+    }
+  }
+}
+
+// Delta-stepping with asynchronous buckets.  Needs every vertex light
+// (degree <= a.heavy, < 65536) and offsets below 2^48 (entries pack them).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) sssp_async(SsspArgs a) {
+  __shared__ uint4 s_lq[BLOCK / 32][kAsyncLQ];
+  SsspCtl* ctl = a.ctl;
+  RingCtl* rc = a.ring.rc;
+  const unsigned nblocks = gridDim.x;
+  const uint64_t deadline = kernel_deadline();
+  const uint32_t lane = lane_id();
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  uint4* lq = s_lq[threadIdx.x >> 5];
+  unsigned long long my_scanned = 0, my_relax = 0;
+
+  uint32_t bucket = 0;
+  int fp = 0;
+  uint32_t P = 0;  // buckets processed
+  for (;;) {
+    if (P >= a.max_phases) {
+      if (gtid == 0) raise_err(&ctl->err, kDevMaxRounds);
+      break;
+    }
+    const uint64_t hi64 = ((uint64_t)bucket + 1) << a.shift;
+    const uint32_t hi = hi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)hi64;
+    uint32_t* farq = a.far[fp];
+    // ---- the bucket's work, no grid barrier --------------------------------
+    uint32_t lq_n = 0;   // warp-uniform local queue length
+    bool busy = false;   // this warp holds one count of rc->work
+    // Relax arc (v -> u) to nd: near improvements go to the local queue, the
+    // ones that do not fit to the ring; far ones to the far pile (once, by
+    // the bitmap).  The target's offsets load beside the atomic.
+    auto relax = [&](bool valid, uint32_t u, uint32_t nd) {
+      bool near = false, far = false;
+      uint64_t ub = 0, deg = 0;
+      if (valid) {
+        ub = ldg(a.offs + u);
+        deg = ldg(a.offs + u + 1) - ub;
+        const uint32_t old = atomicMin(&a.dist[u], nd);
+        if (nd < old) {
+          ++my_relax;
+          if (nd < hi) {
+            near = deg > 0;  // nothing to relax from a vertex without arcs
+          } else {
+            const uint32_t bit = 1u << (u & 31);
+            if (!(a.infar[u >> 5] & bit)) far = !(atomicOr(&a.infar[u >> 5], bit) & bit);
+          }
+        }
+      }
+      const unsigned nm = __ballot_sync(kFull, near);
+      if (nm) {
+        const uint32_t k = __popc(nm), room = kAsyncLQ - lq_n, rank = __popc(nm & lanemask_lt);
+        const uint4 e = make_uint4(u, nd, (uint32_t)ub, (uint32_t)((ub >> 32) << 16) | (uint32_t)deg);
+        const bool loc = near && rank < room;
+        if (loc) lq[lq_n + rank] = e;
+        lq_n += min(k, room);
+        __syncwarp();
+        if (k > room) ring_publish(a.ring, near && !loc, e, &ctl->err);
+      }
+      warp_push(far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
+    };
+    for (;;) {
+      uint4 ent = make_uint4(0u, 0u, 0u, 0u);
+      bool has = false;
+      if (lq_n > 0) {
+        const uint32_t take = min(32u, lq_n);
+        has = lane < take;
+        if (has) ent = lq[lq_n - take + lane];
+        __syncwarp();
+        lq_n -= take;
+      } else {
+        // out of work: give up this warp's count, take a ticket, wait for its chunk
+        if (busy && lane == 0) atomicSub(&rc->work, 1);
+        busy = false;
+        unsigned long long p = 0;
+        int got = 0;
+        if (lane == 0) {
+          p = atomicAdd(&rc->head, 1ull);
+          got = ring_wait(a.ring, p, &ctl->err, deadline);
+        }
+        got = __shfl_sync(kFull, got, 0);
+        if (got <= 0) break;  // the bucket is done (or an error was raised)
+        p = __shfl_sync(kFull, p, 0);
+        __syncwarp();  // lane 0's acquire orders the other lanes' reads below
+        busy = true;   // the chunk's count is now this warp's
+        const unsigned long long slot = p & a.ring.mask;
+        const uint32_t c = __ldcg(a.ring.cnt + slot);
+        has = lane < c;
+        if (has) ent = __ldcg(a.ring.ent + slot * 32 + lane);
+        __syncwarp();
+        if (lane == 0) st_release_u64(a.ring.seq + slot, p + a.ring.mask + 1);  // free for the next lap
+      }
+      // one round: every lane's vertex, its arcs spread over the warp; an
+      // entry whose vertex has a smaller distance by now is stale (whoever
+      // lowered it routed the vertex again)
+      const uint64_t b = ((uint64_t)(ent.w >> 16) << 32) | ent.z;
+      const uint32_t d = has ? (ent.w & 0xFFFFu) : 0u;
+      const uint32_t cur = has ? __ldcg(a.dist + ent.x) : 0u;
+      my_scanned += d;
+      warp_expand_mlp<4, uint32_t>(
+          b, d, ent.y, [&](bool valid, uint64_t e, uint32_t) { return valid ? ldg(a.col + e) : 0u; },
+          [&](bool valid, uint64_t e, uint32_t, uint32_t dsrc) { return valid ? dsrc + ldg(a.w + e) : 0u; },
+          [&](bool valid, uint32_t owner, uint32_t dsrc, uint32_t u, uint32_t nd) {
+            const bool live = __shfl_sync(kFull, cur, owner) >= dsrc;
+            relax(valid && live, u, nd);
+          });
+      // while other warps wait for work, hand them this warp's oldest entries
+      if (lq_n > 32) {
+        int want = 0;
+        if (lane == 0) want = ld_volatile_u64(&rc->head) > ld_volatile_u64(&rc->tail);
+        if (__shfl_sync(kFull, want, 0)) {
+          const uint4 e = lq[lane];
+          __syncwarp();
+          for (uint32_t i = 32 + lane; i < lq_n; i += 32) lq[i - 32] = lq[i];
+          __syncwarp();
+          lq_n -= 32;
+          ring_publish(a.ring, true, e, &ctl->err);
+        }
+      }
+    }
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    // ---- bucket transition ---------------------------------------------------
+    const uint32_t nfar = min(ctl->far_count[fp], a.n);
+    ++P;
+    if (nfar == 0) break;  // nothing left anywhere
+    if (gtid == 0) {
+      rc->head = rc->tail;  // tickets still waiting when the bucket ended are void
+      ctl->min_bucket = 0xFFFFFFFFu;
+      ctl->buckets += 1;
+      ctl->far_count[fp ^ 1] = 0;
+    }
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    // R1: minimum bucket among far entries not yet settled
+    {
+      uint32_t mb = 0xFFFFFFFFu;
+      for (uint64_t i = gtid; i < nfar; i += gthreads) {
+        const uint32_t dd = a.dist[farq[i]];
+        if (dd >= hi) mb = min(mb, dd >> a.shift);
+      }
+      mb = __reduce_min_sync(kFull, mb);
+      if (lane == 0 && mb != 0xFFFFFFFFu) atomicMin(&ctl->min_bucket, mb);
+    }
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    const uint32_t nb = ctl->min_bucket;
+    if (nb == 0xFFFFFFFFu) break;  // every far entry was settled
+    // R2: the entries of bucket nb become chunks, later ones stay in the pile
+    {
+      const uint64_t nhi64 = ((uint64_t)nb + 1) << a.shift;
+      const uint32_t nhi = nhi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)nhi64;
+      uint32_t* keepq = a.far[fp ^ 1];
+      for (uint64_t base = gtid - lane; base < nfar; base += gthreads) {
+        const uint64_t i = base + lane;
+        bool to_near = false, keep = false;
+        uint32_t u = 0, dd = 0;
+        uint64_t ub = 0, deg = 0;
+        if (i < nfar) {
+          u = farq[i];
+          dd = a.dist[u];
+          if (dd >= hi && dd < nhi) {
+            ub = ldg(a.offs + u);
+            deg = ldg(a.offs + u + 1) - ub;
+            to_near = deg > 0;
+          } else if (dd >= nhi) {
+            keep = true;
+          }
+          if (!keep) atomicAnd(&a.infar[u >> 5], ~(1u << (u & 31)));
+        }
+        ring_publish(a.ring, to_near, make_uint4(u, dd, (uint32_t)ub, (uint32_t)((ub >> 32) << 16) | (uint32_t)deg),
+                     &ctl->err);
+        warp_push(keep, u, keepq, &ctl->far_count[fp ^ 1], a.n, &ctl->err);
+      }
+    }
+    bucket = nb;
+    fp ^= 1;
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+  }
+  my_scanned = warp_sum(my_scanned);
+  my_relax = warp_sum(my_relax);
+  if (lane == 0) {
+    if (my_scanned) atomicAdd(&ctl->scanned, my_scanned);
+    if (my_relax) atomicAdd(&ctl->relax, my_relax);
+  }
+  if (gtid == 0) ctl->phases = P;
+}
+
 __global__ void sssp_reach_kernel(const uint32_t* __restrict__ dist, const uint64_t* __restrict__ offs,
                                   uint32_t n, unsigned long long* out) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -517,6 +844,42 @@ __global__ void sssp_reach_kernel(const uint32_t* __restrict__ dist, const uint6
 
 }  // namespace
 
+// Error word, statistics and the host copy of the distances after the
+// persistent kernel.
+static int finish_sssp(gb_graph* g, const SsspArgs& a, unsigned long long* reach, const KernelTimer& kt, uint32_t launches,
+                uint32_t* dist_out, bool out_dev, gb_stats* stats, cudaStream_t s) {
+  const uint32_t n = g->n;
+  int* pin = static_cast<int*>(g->pinned);
+  GB_CUDA(cudaMemcpyAsync(pin, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (stats) {
+    GB_CUDA(cudaMemsetAsync(reach, 0, 16, s));
+    sssp_reach_kernel<<<g->sm_count * 4, 256, 0, s>>>(a.dist, g->offs, n, reach);
+    SsspCtl* hc = reinterpret_cast<SsspCtl*>(static_cast<char*>(g->pinned) + 256);
+    unsigned long long* hr = reinterpret_cast<unsigned long long*>(static_cast<char*>(g->pinned) + 2048);
+    GB_CUDA(cudaMemcpyAsync(hc, a.ctl, sizeof(SsspCtl), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(hr, reach, 16, cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    *stats = gb_stats{};
+    stats->vertices_reached = hr[0];
+    stats->edges_reached = hr[1];
+    stats->edges_scanned = hc->scanned;
+    stats->relaxations = hc->relax;
+    stats->rounds = hc->phases;
+    stats->buckets = hc->buckets + 1;
+    stats->launches = launches;
+    stats->kernel_ms = kt.ms();
+  }
+  if (!out_dev) {
+    int st = copy_out(dist_out, a.dist, sizeof(uint32_t) * n, s);
+    if (st != GB_OK) return st;
+  }
+  if (stats || !out_dev) {
+    GB_CUDA(cudaStreamSynchronize(s));
+    if (*pin) return dev_err_status(*pin, "gb_sssp_delta");
+  }
+  return GB_OK;
+}
+
 int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_stats* stats,
              cudaStream_t s) {
   if (!g->w) GB_FAIL(GB_ERR_ARG, "gb_sssp_delta: graph has no uint32 edge weights");
@@ -525,28 +888,49 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   const uint32_t n = g->n;
   const uint32_t words = (n + 31) / 32;
   const bool out_dev = is_device_ptr(dist_out);
+  const int local_depth = t.local_depth < 0 ? 0 : t.local_depth;
+  // asynchronous buckets: local queues on and every vertex light (entries
+  // pack the degree in 16 bits and the begin offset in 48)
+  const bool async = t.sssp_async >= 0 && local_depth > 0 && g->max_degree <= t.heavy_degree &&
+                     g->max_degree < 65536 && g->m < (1ull << 48);
   FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
   SweepSched sched{};
-  if (g->max_degree > t.heavy_degree) {  // heavy rows of a bitmap frontier come from the tile schedule
+  if (!async && g->max_degree > t.heavy_degree) {  // heavy rows of a bitmap frontier come from the tile schedule
     int sst = ensure_sweep_schedule(g, t.heavy_degree, t.tile_edges, s, &sched);
     if (sst != GB_OK) return sst;
   }
-  const size_t need = carve_size<SsspCtl>(1) + carve_size<uint32_t>(n) + 4 * carve_size<uint32_t>(words) +
-                      2 * carve_size<uint32_t>(n) + fl.bytes + (out_dev ? 0 : carve_size<uint32_t>(n)) +
-                      carve_size<unsigned long long>(2);
+  // ring of chunks: at least n/32 + 8192 positions (a bucket's split fills at
+  // most one chunk per 32 far entries), a power of two
+  uint64_t cap = 1;
+  while (cap < (uint64_t)n / 32 + 8192) cap <<= 1;
+  size_t need = carve_size<SsspCtl>(1) + carve_size<uint32_t>(words) + 2 * carve_size<uint32_t>(n) +
+                (out_dev ? 0 : carve_size<uint32_t>(n)) + carve_size<unsigned long long>(2);
+  if (async)
+    need += carve_size<RingCtl>(1) + carve_size<uint4>(cap * 32) + carve_size<unsigned long long>(cap) +
+            carve_size<uint32_t>(cap);
+  else
+    need += carve_size<uint32_t>(n) + 3 * carve_size<uint32_t>(words) + fl.bytes;
   int st = ws_reserve(g, need, s);
   if (st != GB_OK) return st;
   Carver cv(g->ws);
   SsspArgs a{};
   a.ctl = cv.take<SsspCtl>(1);
-  a.stamp = cv.take<uint32_t>(n);
   a.infar = cv.take<uint32_t>(words);
-  for (int i = 0; i < 3; ++i) a.act[i] = cv.take<uint32_t>(words);
   a.far[0] = cv.take<uint32_t>(n);
   a.far[1] = cv.take<uint32_t>(n);
-  a.fq = carve_frontier(cv, fl);
   unsigned long long* reach = cv.take<unsigned long long>(2);
   a.dist = out_dev ? dist_out : cv.take<uint32_t>(n);
+  if (async) {
+    a.ring.rc = cv.take<RingCtl>(1);
+    a.ring.ent = cv.take<uint4>(cap * 32);
+    a.ring.seq = cv.take<unsigned long long>(cap);
+    a.ring.cnt = cv.take<uint32_t>(cap);
+    a.ring.mask = cap - 1;
+  } else {
+    a.stamp = cv.take<uint32_t>(n);
+    for (int i = 0; i < 3; ++i) a.act[i] = cv.take<uint32_t>(words);
+    a.fq = carve_frontier(cv, fl);
+  }
   a.offs = g->offs;
   a.col = g->col;
   a.w = g->w;
@@ -556,7 +940,7 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   a.heavy = t.heavy_degree;
   a.tile = t.tile_edges;
   a.max_phases = 0x7FFFFFFFu;
-  a.local_depth = t.local_depth < 0 ? 0 : t.local_depth;
+  a.local_depth = local_depth;
   a.all_light = g->max_degree <= t.heavy_degree ? 1 : 0;
   a.sw_tiles = sched.tiles;
   a.sw_ntiles = sched.ntiles;
@@ -565,6 +949,20 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   // beside what such a frontier relaxes (n/64 and n/1024 measured slower on
   // RMAT-22/24)
   a.bm_min = n >> 8;
+  if (async) {
+    GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), s));
+    GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(RingCtl), s));
+    sssp_async_init<<<g->sm_count * 4, 256, 0, s>>>(a);
+    GB_CUDA(cudaGetLastError());
+    const void* kfn = reinterpret_cast<const void*>(&sssp_async<256>);
+    const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
+    if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
+    void* args[] = {&a};
+    KernelTimer kt(stats != nullptr, s);
+    GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, args, 0, s));
+    kt.stop(s);
+    return finish_sssp(g, a, reach, kt, 2, dist_out, out_dev, stats, s);
+  }
   GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), s));
   sssp_init<<<g->sm_count * 4, 256, 0, s>>>(a);
   GB_CUDA(cudaGetLastError());
@@ -586,35 +984,7 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   KernelTimer kt(stats != nullptr, s);
   GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, block, args, 0, s));
   kt.stop(s);
-  int* pin = static_cast<int*>(g->pinned);
-  GB_CUDA(cudaMemcpyAsync(pin, &a.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
-  if (stats) {
-    GB_CUDA(cudaMemsetAsync(reach, 0, 16, s));
-    sssp_reach_kernel<<<g->sm_count * 4, 256, 0, s>>>(a.dist, g->offs, n, reach);
-    SsspCtl* hc = reinterpret_cast<SsspCtl*>(static_cast<char*>(g->pinned) + 256);
-    unsigned long long* hr = reinterpret_cast<unsigned long long*>(static_cast<char*>(g->pinned) + 2048);
-    GB_CUDA(cudaMemcpyAsync(hc, a.ctl, sizeof(SsspCtl), cudaMemcpyDeviceToHost, s));
-    GB_CUDA(cudaMemcpyAsync(hr, reach, 16, cudaMemcpyDeviceToHost, s));
-    GB_CUDA(cudaStreamSynchronize(s));
-    *stats = gb_stats{};
-    stats->vertices_reached = hr[0];
-    stats->edges_reached = hr[1];
-    stats->edges_scanned = hc->scanned;
-    stats->relaxations = hc->relax;
-    stats->rounds = hc->phases;
-    stats->buckets = hc->buckets + 1;
-    stats->launches = 2;
-    stats->kernel_ms = kt.ms();
-  }
-  if (!out_dev) {
-    st = copy_out(dist_out, a.dist, sizeof(uint32_t) * n, s);
-    if (st != GB_OK) return st;
-  }
-  if (stats || !out_dev) {
-    GB_CUDA(cudaStreamSynchronize(s));
-    if (*pin) return dev_err_status(*pin, "gb_sssp_delta");
-  }
-  return GB_OK;
+  return finish_sssp(g, a, reach, kt, 2, dist_out, out_dev, stats, s);
 }
 
 }  // namespace gb

@@ -148,6 +148,14 @@ class DeviceGraph:
         to graph.assign_weights_u32 on the host for the same arcs and seed."""
         check(lib.gb_graph_assign_weights_u32(self.handle, lo, hi, seed, None), "gb_graph_assign_weights_u32")
 
+    def assign_weights_reference(self, min_value: int = 1, max_value: int = 100, dtype: str = "u32") -> None:
+        """gr2randomweightgr's weights (a default std::mt19937, arc order) on
+        the device mirror; see galois_b200.graph.assign_weights_reference."""
+        if dtype not in ("u32", "f32"):
+            raise ValueError("dtype must be 'u32' or 'f32'")
+        check(lib.gb_graph_assign_weights_reference(self.handle, min_value, max_value, 4 if dtype == "u32" else -4,
+                                                    None), "gb_graph_assign_weights_reference")
+
     def assign_weights_f32(self, seed: int) -> None:
         check(lib.gb_graph_assign_weights_f32(self.handle, seed, None), "gb_graph_assign_weights_f32")
 

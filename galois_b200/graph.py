@@ -169,6 +169,27 @@ def assign_weights_f32(g: HostCSR, seed: int = 1) -> HostCSR:
     return g
 
 
+def assign_weights_reference(g: HostCSR, min_value: int = 1, max_value: int = 100, dtype: str = "u32") -> HostCSR:
+    """Weights as the reference's gr2randomweightgr draws them: a default
+    std::mt19937 with a uniform int (dtype "u32") or float ("f32")
+    distribution over [min_value, max_value], one draw per arc in arc order
+    (graph-convert.cpp:1145-1190; the converter's defaults are 1 and 100)."""
+    if dtype not in ("u32", "f32"):
+        raise ValueError("dtype must be 'u32' or 'f32'")
+    c = g._as_c()
+    c.w_u32 = C.POINTER(C.c_uint32)()
+    c.w_f32 = C.POINTER(C.c_float)()
+    eb = 4 if dtype == "u32" else -4
+    check(lib.gb_assign_weights_reference(C.byref(c), min_value, max_value, eb), "gb_assign_weights_reference")
+    if dtype == "u32":
+        g.w_u32 = _np_from(c.w_u32, g.m, np.uint32)
+        _free_ptr(c.w_u32)
+    else:
+        g.w_f32 = _np_from(c.w_f32, g.m, np.float32)
+        _free_ptr(c.w_f32)
+    return g
+
+
 def _free_ptr(p) -> None:
     libc = C.CDLL(None)
     libc.free.argtypes = [C.c_void_p]

@@ -118,6 +118,16 @@ int gb_gen_er(uint32_t n, double mean_degree, uint64_t seed, gb_host_csr* out);
 int gb_assign_weights_u32(gb_host_csr* g, uint32_t lo, uint32_t hi,
                           uint64_t seed);
 int gb_assign_weights_f32(gb_host_csr* g, uint64_t seed);
+/* gr2randomweightgr as the reference converter draws it
+ * (tools/graph-convert/graph-convert.cpp:1145-1190): a default-constructed
+ * std::mt19937 and std::uniform_int_distribution<uint32_t>(min_value,
+ * max_value) (edge_bytes 4, into w_u32) or
+ * std::uniform_real_distribution<float>(min_value, max_value) (edge_bytes -4,
+ * into w_f32), one draw per arc in arc order (the converter's defaults are
+ * min 1, max 100).  Serial, from the C++ standard library this library was
+ * built with. */
+int gb_assign_weights_reference(gb_host_csr* g, int min_value, int max_value,
+                                int edge_bytes);
 /* Transpose (LC_CSR_Graph.h:617-712 semantics): arcs u->v become v->u, edge
  * data follows its arc, adjacency sorted by source id.  If edge_map is
  * non-NULL it receives, for every transposed arc, its index in g. */
@@ -167,6 +177,10 @@ int gb_graph_build_transpose(gb_graph* g, void* stream);
  * generators, so the result equals gb_assign_weights_u32 / _f32 on the same
  * arcs and seed (uniform in [lo, hi]; fp32 in (0, 1]). */
 int gb_graph_symmetrize(gb_graph* g, int cleanup, void* stream);
+/* gb_assign_weights_reference on the device mirror's arcs (drawn on the host
+ * in arc order, then uploaded; synchronous).  Before gb_graph_reorder. */
+int gb_graph_assign_weights_reference(gb_graph* g, int min_value, int max_value,
+                                      int edge_bytes, void* stream);
 int gb_graph_assign_weights_u32(gb_graph* g, uint32_t lo, uint32_t hi,
                                 uint64_t seed, void* stream);
 int gb_graph_assign_weights_f32(gb_graph* g, uint64_t seed, void* stream);
@@ -218,6 +232,10 @@ typedef struct gb_tuning {
   int direction_opt;     /* 0 = pull steps allowed when in-edges exist, 2 = push only */
   int local_depth;       /* SSSP: per-warp local-queue rounds per phase
                             (0 = library default, < 0 = off) */
+  int sssp_async;        /* SSSP with local queues on a graph whose every
+                            vertex is light: 0 = library default
+                            (asynchronous buckets), < 0 = a grid barrier
+                            after every phase */
 } gb_tuning;
 int gb_graph_set_tuning(gb_graph* g, const gb_tuning* t);
 int gb_graph_get_tuning(const gb_graph* g, gb_tuning* t);

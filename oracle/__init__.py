@@ -69,6 +69,8 @@ _SIG = {
     "orc_bc_level_f64": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
     "orc_bc_level_par": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
     "orc_bc_level_f64_par_sources": (None, [_u32, _vp, _vp, _vp, _u32, _vp]),
+    "orc_gr2randomweight": (None, [C.c_uint64, C.c_int, C.c_int, C.c_int, _vp]),
+    "orc_mt19937_raw": (None, [C.c_uint64, _vp]),
     "orc_ppr_solve_f64": (_u32, [_u32, _vp, _vp, _vp, _vp, C.c_double, C.c_double, _u32, C.c_int, _vp]),
 }
 for _n, (_r, _a) in _SIG.items():
@@ -327,3 +329,18 @@ def ppr_solve_f64(g, w, rhs, alpha=0.85, tol=1e-13, max_iter=10000, adjoint=Fals
     it = _lib.orc_ppr_solve_f64(n, _p(end), _p(col), _p(wf), _p(r), alpha, tol, max_iter, 1 if adjoint else 0,
                                 _p(out))
     return out, int(it)
+
+
+def gr2randomweight(m: int, lo: int = 1, hi: int = 100, dtype: str = "u32") -> np.ndarray:
+    """The weights graph-convert's gr2randomweightgr writes for m arcs
+    (graph-convert.cpp:1145-1190), from the C++ standard library."""
+    out = np.empty(m, np.uint32)
+    _lib.orc_gr2randomweight(m, lo, hi, 1 if dtype == "f32" else 0, _p(out))
+    return out.view(np.float32) if dtype == "f32" else out
+
+
+def mt19937_raw(count: int) -> np.ndarray:
+    """The first `count` outputs of a default-constructed std::mt19937."""
+    out = np.empty(count, np.uint32)
+    _lib.orc_mt19937_raw(count, _p(out))
+    return out

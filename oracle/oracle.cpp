@@ -29,6 +29,7 @@
 #include <deque>
 #include <functional>
 #include <queue>
+#include <random>
 #include <vector>
 
 namespace {
@@ -477,6 +478,31 @@ int orc_verify_cc(uint32_t n, const uint64_t* end, const uint32_t* col, const ui
     for (uint64_t i = g.b(v); i < g.e(v); ++i)
       if (label[col[i]] != label[v]) return 1;
   return 0;
+}
+
+// RandomizeEdgeWeights (tools/graph-convert/graph-convert.cpp:1145-1190):
+// a default-constructed std::mt19937, one uniform draw per arc in arc order,
+// std::uniform_int_distribution<uint32_t>(lo, hi) or, with is_float,
+// std::uniform_real_distribution<float>(lo, hi) written as float bits.
+void orc_gr2randomweight(uint64_t m, int lo, int hi, int is_float, uint32_t* out) {
+  std::mt19937 gen;
+  if (is_float) {
+    std::uniform_real_distribution<float> dist((float)lo, (float)hi);
+    for (uint64_t e = 0; e < m; ++e) {
+      const float x = dist(gen);
+      std::memcpy(out + e, &x, 4);
+    }
+  } else {
+    std::uniform_int_distribution<uint32_t> dist((uint32_t)lo, (uint32_t)hi);
+    for (uint64_t e = 0; e < m; ++e) out[e] = dist(gen);
+  }
+}
+
+// The raw output of a default-constructed std::mt19937 (the C++ standard,
+// [rand.predef], fixes its 10000th value at 4123659995).
+void orc_mt19937_raw(uint64_t count, uint32_t* out) {
+  std::mt19937 gen;
+  for (uint64_t i = 0; i < count; ++i) out[i] = (uint32_t)gen();
 }
 
 }  // extern "C"

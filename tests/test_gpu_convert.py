@@ -76,3 +76,23 @@ def test_device_weights_equal_host_generator(cuda_device):
         assert (dg.sssp(src, 13) == oracle.sssp_dijkstra(host, src)).all()
         with pytest.raises(GbError):
             dg.assign_weights_u32(9, 3, 1)
+
+
+def test_device_reference_weights_equal_converter_draws(cuda_device):
+    """gb_graph_assign_weights_reference: the draws of gr2randomweightgr (a
+    default std::mt19937 in arc order, graph-convert.cpp:1145-1190) on the
+    device mirror, equal to the oracle's restatement; SSSP then runs on them."""
+    g, perm = rmat(11, 8, seed=5, symmetrize=False)
+    src = int(perm[0])
+    with DeviceGraph(HostCSR(g.end_offs, g.col)) as dg:
+        dg.assign_weights_reference(1, 100, "u32")
+        dg.assign_weights_reference(1, 100, "f32")
+        _, _, w, wf = dg.to_host()
+        assert np.array_equal(w, oracle.gr2randomweight(g.m, 1, 100, "u32"))
+        assert np.array_equal(wf.view(np.uint32), oracle.gr2randomweight(g.m, 1, 100, "f32").view(np.uint32))
+        host = HostCSR(g.end_offs, g.col, w_u32=w)
+        assert (dg.sssp(src, 13) == oracle.sssp_dijkstra(host, src)).all()
+        dg.reorder()
+        with pytest.raises(GbError) as e:
+            dg.assign_weights_reference(1, 100)
+        assert e.value.status == _lib.GB_ERR_UNSUPPORTED

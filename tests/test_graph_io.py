@@ -170,3 +170,50 @@ def test_host_transpose():
     assert np.array_equal(g.w_u32[emap], t.w_u32)
     tt, _ = transpose(t)
     assert np.array_equal(tt.col, g.col) and np.array_equal(tt.end_offs, g.end_offs)
+
+
+def test_mt19937_known_answer():
+    """The oracle's generator is the standard's: the 10000th output of a
+    default-constructed std::mt19937 is 4123659995 ([rand.predef])."""
+    import oracle
+
+    assert int(oracle.mt19937_raw(10000)[-1]) == 4123659995
+
+
+@pytest.mark.parametrize("dtype,lo,hi", [("u32", 1, 100), ("u32", 1, 255), ("f32", 1, 100)])
+def test_reference_random_weights_gr(tmp_path, dtype, lo, hi):
+    """gr2randomweightgr (graph-convert.cpp:1145-1190): a .gr written with
+    assign_weights_reference carries, in arc order, the draws of a default
+    std::mt19937 through the uniform distribution the converter uses."""
+    import oracle
+    from galois_b200 import assign_weights_reference
+
+    g, _ = rmat(9, 8, seed=3, symmetrize=False)
+    assign_weights_reference(g, lo, hi, dtype)
+    eb = 4 if dtype == "u32" else -4
+    p = tmp_path / "w.gr"
+    write_gr(p, g, eb)
+    raw = p.read_bytes()
+    ver, szedge, n, m = struct.unpack_from("<4Q", raw, 0)
+    assert (ver, szedge, n, m) == (1, 4, g.n, g.m)
+    data_off = 32 + 8 * n + 4 * m + (4 if m % 2 else 0)
+    got = np.frombuffer(raw, dtype=np.uint32, count=m, offset=data_off)
+    want = oracle.gr2randomweight(m, lo, hi, dtype)
+    assert np.array_equal(got, want.view(np.uint32))
+    if dtype == "u32":
+        assert got.min() >= lo and got.max() <= hi
+    else:
+        f = got.view(np.float32)
+        assert f.min() >= lo and f.max() < hi
+    h = read_gr(p, eb)
+    assert np.array_equal(h.w_u32 if dtype == "u32" else h.w_f32.view(np.uint32), want.view(np.uint32))
+
+
+def test_reference_random_weights_rejects_bad_arguments():
+    from galois_b200 import assign_weights_reference
+
+    g = small_graph()
+    with pytest.raises(GbError):
+        assign_weights_reference(g, 5, 1)
+    with pytest.raises(GbError):
+        assign_weights_reference(g, -3, 5, "u32")
