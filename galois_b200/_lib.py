@@ -29,6 +29,8 @@ GB_CC_AFFOREST = 2
 GB_ORDER_NONE = 0
 GB_ORDER_DEGREE = 1
 GB_ORDER_DEGREE_UNSORTED = 2
+GB_PR_PUSH_ASYNC = 0
+GB_PR_PUSH_SYNC = 1
 
 _STATUS_NAMES = {
     GB_ERR_ARG: "GB_ERR_ARG", GB_ERR_OOM: "GB_ERR_OOM", GB_ERR_CUDA: "GB_ERR_CUDA",
@@ -132,6 +134,8 @@ SIGNATURES: dict[str, tuple] = {
     "gb_pagerank_pull_ex": (C.c_int, [_gp, C.c_float, C.c_float, C.c_uint32, C.c_float, C.c_float, C.c_int,
                                       _vp, _u32p, C.POINTER(Stats), _vp]),
     "gb_pagerank_push": (C.c_int, [_gp, C.c_float, C.c_float, C.c_uint32, _vp, _u32p, C.POINTER(Stats), _vp]),
+    "gb_pagerank_push_ex": (C.c_int, [_gp, C.c_int, C.c_float, C.c_float, C.c_uint32, _vp, _u32p, C.POINTER(Stats),
+                                      _vp]),
     "gb_pagerank_pull_residual": (C.c_int, [_gp, C.c_float, C.c_float, C.c_uint32, _vp, _u32p,
                                             C.POINTER(Stats), _vp]),
     "gb_bc": (C.c_int, [_gp, _vp, C.c_uint32, C.c_uint32, _vp, C.POINTER(Stats), _vp]),

@@ -15,6 +15,12 @@
 //                     1-alpha; active vertices over tol absorb their residual
 //                     and push residual*alpha/outdeg along out-edges; a
 //                     vertex is activated when its residual crosses tol.
+//                     PageRank-push.cpp:68-101 (Async, the app's default):
+//                     the same operator over a worklist with no rounds -- a
+//                     vertex is processed when it is taken, absorbing the
+//                     residual accumulated until then (exchange with 0), and
+//                     pushed again when an add lifts its residual from below
+//                     tol to tol or above.
 //
 // B200 design: one cooperative persistent launch per solve.  Pull iterations
 // use the cached all-vertex sweep schedule (sweep.cuh): 32 consecutive
@@ -22,13 +28,17 @@
 // heavy vertices as tiles whose partial sums meet in an accumulator, a
 // contribution array c[u] = value[u]/nout[u] (SoA, double-buffered) so each
 // arc costs one 4-byte column read and one 4-byte gather, and the L1 change
-// reduced in fp64.  Residual push reuses the frontier queues (frontier.cuh).
+// reduced in fp64.  Residual push (Sync) reuses the frontier queues
+// (frontier.cuh); Async runs over the device worklist (gb_worklist.cuh): a
+// warp keeps working on the vertices it activated itself, surplus goes to
+// the ring, and the launch ends when the worklist's work count reaches zero.
 
 #include <algorithm>
 
 #include "device_common.cuh"
 #include "device_graph.cuh"
 #include "frontier.cuh"
+#include "gb_worklist.cuh"
 #include "sweep.cuh"
 
 #include <cstring>
@@ -51,6 +61,7 @@ struct PrCtl {
   uint32_t pad;
   FrontierCounters fc[3];
   unsigned long long pushes;
+  unsigned long long absorbs;  // Async push: residuals taken
 };
 
 struct PrArgs {
@@ -80,6 +91,7 @@ struct PrArgs {
   uint32_t* stamp;
   FrontierQueues fq;
   uint32_t heavy, tile;
+  wl::Ring ring;  // Async push: the worklist ring
   uint32_t zero_from;  // first vertex of the no-in-arc suffix (degree-ordered graphs), else n
   // flat sweep of the light rows (degree-ordered graphs): arcs [lr_arc0,
   // lr_arc1) in runs of kLightRun; an arc's row is lr_runrow[run] +
@@ -615,6 +627,116 @@ __global__ void __launch_bounds__(kBlock) pr_push_persistent(PrArgs a) {
   if (lane == 0 && my_push) atomicAdd(&ctl->pushes, my_push);
 }
 
+// ---- residual push, Async (PageRank-push.cpp:68-101) -------------------------
+// Worklist entries: (v, kAbsorb, 0, 0) "take v's residual if it is above
+// tol" -- every vertex once at the start (the reference iterates the whole
+// graph), then each vertex whose residual an add lifts across tol -- and
+// (v, k, delta bits, 0): "add delta along the k-th tile of v's arcs", made
+// when a heavy vertex is absorbed.
+constexpr uint32_t kAbsorb = 0xFFFFFFFFu;
+constexpr int kPushLQ = 64;
+
+__global__ void pr_push_async_init(PrArgs a, uint32_t nchunks) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = tid; v < a.n; v += stride) {
+    a.value[v] = 0.f;
+    a.residual[v] = 1.0f - a.alpha;  // INIT_RESIDUAL, PageRank-constants.h:33
+  }
+  // the initial worklist: every vertex, 32 per chunk, published
+  for (uint64_t i = tid; i <= a.ring.mask; i += stride) {
+    if (i < nchunks) {
+      const uint32_t first = (uint32_t)(i * 32);
+      const uint32_t cnt = min(32u, a.n - first);
+      for (uint32_t j = 0; j < cnt; ++j) a.ring.ent[i * 32 + j] = make_uint4(first + j, kAbsorb, 0u, 0u);
+      a.ring.cnt[i] = cnt;
+      a.ring.seq[i] = i + 1;
+    } else {
+      a.ring.seq[i] = i;
+    }
+  }
+  if (tid == 0) {
+    a.ring.rc->tail = nchunks;
+    a.ring.rc->work = (int)nchunks;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock, 1) pr_push_async(PrArgs a) {
+  __shared__ uint4 s_lq[kWarps][kPushLQ];
+  PrCtl* ctl = a.ctl;
+  const uint64_t deadline = kernel_deadline();
+  const uint32_t lane = lane_id();
+  unsigned long long my_push = 0, my_absorb = 0;
+  wl::WarpQueue<kPushLQ> q(s_lq[threadIdx.x >> 5], a.ring, &ctl->err, deadline);
+  const float tol = a.tol;
+  // add d to u's residual; activate u when the add lifts it across tol
+  // (old < tol <= old + d, PageRank-push.cpp:92-94)
+  auto add = [&](bool valid, uint32_t u, float d) {
+    bool act = false;
+    if (valid && d > 0.f) {
+      const float old = atomicAdd(&a.residual[u], d);
+      ++my_push;
+      act = old < tol && old + d >= tol;
+    }
+    q.push(act, make_uint4(u, kAbsorb, 0u, 0u));
+  };
+  for (;;) {
+    uint4 ent;
+    bool has;
+    const int got = q.next(ent, has);
+    if (got <= 0) break;
+    // tiles of heavy vertices: the whole warp adds along each in turn
+    unsigned tm = __ballot_sync(kFull, has && ent.y != kAbsorb);
+    while (tm) {
+      const int j = __ffs(tm) - 1;
+      tm &= tm - 1u;
+      const uint32_t v = __shfl_sync(kFull, ent.x, j);
+      const uint32_t k = __shfl_sync(kFull, ent.y, j);
+      const float d = __uint_as_float(__shfl_sync(kFull, ent.z, j));
+      const uint64_t vb = ldg(a.offs + v), ve = ldg(a.offs + v + 1);
+      const uint64_t b = vb + (uint64_t)k * a.tile, e_end = min(ve, b + a.tile);
+      for (uint64_t e0 = b; e0 < e_end; e0 += 32) {
+        const uint64_t e = e0 + lane;
+        add(e < e_end, e < e_end ? ldg(a.col + e) : 0u, d);
+      }
+    }
+    // absorb: exchange the residual with 0 if it is above tol
+    const bool absorb = has && ent.y == kAbsorb;
+    uint64_t b = 0, deg = 0;
+    float delta = 0.f;
+    if (absorb && __ldcg(a.residual + ent.x) > tol) {
+      const float old = atomicExch(&a.residual[ent.x], 0.f);
+      atomicAdd(&a.value[ent.x], old);  // a vertex may be queued twice when tol >= 1 - alpha
+      ++my_absorb;
+      b = ldg(a.offs + ent.x);
+      deg = ldg(a.offs + ent.x + 1) - b;
+      if (deg > 0) delta = old * a.alpha / (float)deg;
+    }
+    const bool light = deg > 0 && deg <= a.heavy;
+    // light rows: their arcs spread over the warp
+    warp_expand(b, light ? (uint32_t)deg : 0u, __float_as_uint(delta), [&](bool valid, uint64_t e, uint32_t, uint32_t pl) {
+      add(valid, valid ? ldg(a.col + e) : 0u, __uint_as_float(pl));
+    });
+    // heavy rows: one worklist entry per tile
+    unsigned hm = __ballot_sync(kFull, deg > a.heavy && delta > 0.f);
+    while (hm) {
+      const int j = __ffs(hm) - 1;
+      hm &= hm - 1u;
+      const uint32_t v = __shfl_sync(kFull, ent.x, j);
+      const uint32_t nt = (uint32_t)((__shfl_sync(kFull, deg, j) + a.tile - 1) / a.tile);
+      const uint32_t dbits = __shfl_sync(kFull, __float_as_uint(delta), j);
+      for (uint32_t t0 = 0; t0 < nt; t0 += 32) q.push(t0 + lane < nt, make_uint4(v, t0 + lane, dbits, 0u));
+    }
+    q.share();
+  }
+  my_push = warp_sum(my_push);
+  my_absorb = warp_sum(my_absorb);
+  if (lane == 0) {
+    if (my_push) atomicAdd(&ctl->pushes, my_push);
+    if (my_absorb) atomicAdd(&ctl->absorbs, my_absorb);
+  }
+}
+
 int ensure_nout(gb_graph* g, cudaStream_t s) {
   if (g->outdeg_of_stored) return GB_OK;
   GB_CUDA(cudaMalloc(&g->outdeg_of_stored, sizeof(uint32_t) * g->n));
@@ -624,7 +746,7 @@ int ensure_nout(gb_graph* g, cudaStream_t s) {
   return GB_OK;
 }
 
-enum class PrKind { Pull, PullResidual, Push };
+enum class PrKind { Pull, PullResidual, Push, PushAsync };
 
 inline float bits_to_float(uint32_t u) {
   float f;
@@ -644,16 +766,21 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
   const bool out_dev = is_device_ptr(rank_out);
   int st = GB_OK;
   SweepSched sched{};
-  if (kind != PrKind::Push) {
+  if (kind == PrKind::Pull || kind == PrKind::PullResidual) {
     st = ensure_sweep_schedule(g, t.heavy_degree, t.tile_edges, s, &sched);
     if (st != GB_OK) return st;
     st = ensure_nout(g, s);
     if (st != GB_OK) return st;
   }
   FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
+  // Async: the initial worklist (every vertex, 32 per chunk) plus room for
+  // as many chunks again and the tiles of the heavy vertices
+  const uint32_t nchunks = (uint32_t)(((uint64_t)n + 31) / 32);
+  const unsigned long long cap = wl::ring_capacity(2ull * nchunks + g->m / ((uint64_t)t.tile_edges * 32) + 8192);
   size_t need = carve_size<PrCtl>(1) + 5 * carve_size<float>(n) + (out_dev ? 0 : carve_size<float>(n));
   if (kind != PrKind::Pull) need += 2 * carve_size<float>(n);
   if (kind == PrKind::Push) need += 3 * carve_size<uint32_t>(n) + fl.bytes;
+  if (kind == PrKind::PushAsync) need += carve_size<char>(wl::ring_bytes(cap));
   st = ws_reserve(g, need, s);
   if (st != GB_OK) return st;
   Carver cv(g->ws);
@@ -673,6 +800,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
     a.stamp = cv.take<uint32_t>(n);
     a.fq = carve_frontier(cv, fl);
   }
+  if (kind == PrKind::PushAsync) a.ring = wl::ring_layout(cv.take<char>(wl::ring_bytes(cap)), cap);
   a.value = out_dev ? rank_out : cv.take<float>(n);
   a.offs = g->offs;
   a.col = g->col;
@@ -732,9 +860,13 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
     pr_resid_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     GB_CUDA(cudaMemsetAsync(a.acc, 0, sizeof(float) * n, s));
     kfn = reinterpret_cast<const void*>(&pr_pull_residual_persistent);
-  } else {
+  } else if (kind == PrKind::Push) {
     pr_push_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     kfn = reinterpret_cast<const void*>(&pr_push_persistent);
+  } else {
+    GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(wl::RingCtl), s));
+    pr_push_async_init<<<g->sm_count * 4, 256, 0, s>>>(a, nchunks);
+    kfn = reinterpret_cast<const void*>(&pr_push_async);
   }
   GB_CUDA(cudaGetLastError());
   const int grid = coop_grid(g, kfn, kBlock, 0, t.blocks_per_sm);
@@ -752,6 +884,8 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
   if (stats || iters_out || !out_dev) {
     GB_CUDA(cudaStreamSynchronize(s));
     if (hc->err) return dev_err_status(hc->err, "pagerank");
+    // Async has no rounds: one pass over the worklist
+    if (kind == PrKind::PushAsync) hc->iters = 1;
     if (iters_out) *iters_out = hc->iters;
     if (stats) {
       *stats = gb_stats{};
@@ -759,6 +893,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
       stats->edges_reached = g->m;
       stats->rounds = hc->iters;
       stats->relaxations = hc->pushes;
+      if (kind == PrKind::PushAsync) stats->vertices_reached = hc->absorbs;  // residuals taken
       stats->launches = 2;
       stats->kernel_ms = kt.ms();
       double l1sum = 0.0;
@@ -766,7 +901,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
       stats->residual = kind == PrKind::Pull ? (linf ? (double)bits_to_float(hc->linf[(hc->iters + 2) % 3]) : l1sum)
                                              : 0.0;
     }
-    if (kind != PrKind::Push && hc->iters >= max_iter) {
+    if (kind != PrKind::Push && kind != PrKind::PushAsync && hc->iters >= max_iter) {
       // the ranks are set; the status tells the caller the cap was hit
       gb::set_error("pagerank: failed to converge in %u iterations", hc->iters);
       return GB_ERR_NOT_CONVERGED;
@@ -832,6 +967,16 @@ int gb_pagerank_push(gb_graph* g, float alpha, float tol, uint32_t max_iter, flo
   GB_CUDA(cudaSetDevice(g->device));
   return gb::pagerank_entry(g, gb::PrKind::Push, alpha, tol, max_iter, rank_out, iters_out, stats,
                             static_cast<cudaStream_t>(stream));
+}
+
+int gb_pagerank_push_ex(gb_graph* g, int algo, float alpha, float tol, uint32_t max_iter, float* rank_out,
+                        uint32_t* iters_out, gb_stats* stats, void* stream) {
+  gb::clear_error();
+  if (!g || !rank_out) GB_FAIL(GB_ERR_ARG, "gb_pagerank_push_ex: null argument");
+  if (algo != GB_PR_PUSH_ASYNC && algo != GB_PR_PUSH_SYNC) GB_FAIL(GB_ERR_ARG, "gb_pagerank_push_ex: unknown algo %d", algo);
+  GB_CUDA(cudaSetDevice(g->device));
+  return gb::pagerank_entry(g, algo == GB_PR_PUSH_ASYNC ? gb::PrKind::PushAsync : gb::PrKind::Push, alpha, tol,
+                            max_iter, rank_out, iters_out, stats, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

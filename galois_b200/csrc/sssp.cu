@@ -637,9 +637,31 @@ __global__ void sssp_async_init(SsspArgs a) {
   }
 }
 
+// Bitonic sort of one 64-bit value per lane across the warp (ascending or
+// descending by lane).
+__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v, bool ascending) {
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (uint32_t k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      const unsigned long long o = __shfl_xor_sync(kFull, v, j);
+      // the k-block runs up (ascending) or down; its lower lane of each pair
+      // keeps the minimum when the block runs up
+      const bool up = ((lane & k) == 0) == ascending;
+      const bool take_min = ((lane & j) == 0) == up;
+      v = take_min ? (o < v ? o : v) : (o > v ? o : v);
+    }
+  }
+  return v;
+}
+
 // Delta-stepping with asynchronous buckets.  Needs every vertex light
 // (degree <= a.heavy, < 65536) and offsets below 2^48 (entries pack them).
-template <int BLOCK>
+// kMode bit 0: prefetch the arcs of every vertex queued (into L2) while its
+// entry waits; bit 1: a round takes the 32 queued entries of smallest
+// distance instead of the 32 most recent.
+template <int BLOCK, int kMode>
 __global__ void __launch_bounds__(BLOCK) sssp_async(SsspArgs a) {
   __shared__ uint4 s_lq[BLOCK / 32][kAsyncLQ];
   SsspCtl* ctl = a.ctl;
@@ -696,13 +718,34 @@ __global__ void __launch_bounds__(BLOCK) sssp_async(SsspArgs a) {
         lq_n += min(k, room);
         __syncwarp();
         if (k > room) ring_publish(a.ring, near && !loc, e, &ctl->err);
+        if ((kMode & 1) && near) {
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a.col + ub));
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a.w + ub));
+        }
       }
       warp_push(far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
     };
     for (;;) {
       uint4 ent = make_uint4(0u, 0u, 0u, 0u);
       bool has = false;
-      if (lq_n > 0) {
+      if ((kMode & 2) && lq_n > 32) {
+        // the 32 entries of smallest distance: sort the first 32 up and the
+        // rest down; the lane-wise minima are the 32 smallest of all
+        const bool hb = lane + 32 < lq_n;
+        const unsigned long long ka = ((unsigned long long)lq[lane].y << 32) | lane;
+        const unsigned long long kb = hb ? ((unsigned long long)lq[lane + 32].y << 32) | (lane + 32) : ~0ull;
+        const unsigned long long sa = warp_sort32(ka, true), sb = warp_sort32(kb, false);
+        const unsigned long long mine = sa < sb ? sa : sb, rest = sa < sb ? sb : sa;
+        ent = lq[(uint32_t)mine & 63u];
+        has = true;
+        const bool keep = rest != ~0ull;
+        const uint4 kept = keep ? lq[(uint32_t)rest & 63u] : make_uint4(0u, 0u, 0u, 0u);
+        __syncwarp();
+        const unsigned km = __ballot_sync(kFull, keep);
+        if (keep) lq[__popc(km & lanemask_lt)] = kept;
+        __syncwarp();
+        lq_n -= 32;
+      } else if (lq_n > 0) {
         const uint32_t take = min(32u, lq_n);
         has = lane < take;
         if (has) ent = lq[lq_n - take + lane];
@@ -954,7 +997,12 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
     GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(RingCtl), s));
     sssp_async_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     GB_CUDA(cudaGetLastError());
-    const void* kfn = reinterpret_cast<const void*>(&sssp_async<256>);
+    // sssp_async: 0 = library default, 1..4 = kernel variants 0..3 (prefetch, distance order)
+    const int mode = t.sssp_async == 0 ? 3 : (t.sssp_async - 1) & 3;
+    const void* kfn = mode == 0   ? reinterpret_cast<const void*>(&sssp_async<256, 0>)
+                      : mode == 1 ? reinterpret_cast<const void*>(&sssp_async<256, 1>)
+                      : mode == 2 ? reinterpret_cast<const void*>(&sssp_async<256, 2>)
+                                  : reinterpret_cast<const void*>(&sssp_async<256, 3>);
     const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
     if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
     void* args[] = {&a};

@@ -258,8 +258,24 @@ class DeviceGraph:
         return self._pr("gb_pagerank_pull_residual", alpha, tol, max_iter, out, stats, allow_not_converged)
 
     def pagerank_push(self, alpha=0.85, tol=1e-3, max_iter=1000, out=None, stats=False,
-                      allow_not_converged=True):
-        return self._pr("gb_pagerank_push", alpha, tol, max_iter, out, stats, allow_not_converged)
+                      allow_not_converged=True, algo: str = "sync"):
+        """Residual push (PageRank-push.cpp): algo "sync" (rounds, :103-188)
+        or "async" (one worklist pass, :68-101, the lonestar app's default;
+        max_iter does not apply and one iteration is reported)."""
+        if algo == "sync":
+            return self._pr("gb_pagerank_push", alpha, tol, max_iter, out, stats, allow_not_converged)
+        if algo != "async":
+            raise ValueError("algo must be 'sync' or 'async'")
+        ptr, stream, obj = self._out(out, self.n, np.float32, "rank_out")
+        it = C.c_uint32(0)
+        s = Stats()
+        st = lib.gb_pagerank_push_ex(self.handle, _lib.GB_PR_PUSH_ASYNC, alpha, tol, max_iter, ptr, C.byref(it),
+                                     C.byref(s), stream)
+        check(st, "gb_pagerank_push_ex")
+        info = s.as_dict()
+        info["iterations"] = it.value
+        info["converged"] = True
+        return (obj, info) if stats else obj
 
     def bc(self, sources, batch: int = 64, out=None, stats: bool = False):
         src = np.ascontiguousarray(np.asarray(sources, dtype=np.uint32))

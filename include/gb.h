@@ -312,6 +312,17 @@ int gb_pagerank_pull_ex(gb_graph* g, float alpha, float tol, uint32_t max_iter,
 int gb_pagerank_push(gb_graph* g, float alpha, float tol, uint32_t max_iter,
                      float* rank_out, uint32_t* iters_out, gb_stats* stats,
                      void* stream);
+/* Residual push with the algorithm chosen as PageRank-push.cpp:42-47 does:
+ * GB_PR_PUSH_ASYNC (the app's default, :68-101) runs the operator over a
+ * worklist with no rounds -- every vertex at the start, then each vertex
+ * whose residual an add lifts from below tol to tol or above -- and reports
+ * one iteration (max_iter is ignored, as the reference ignores it there);
+ * GB_PR_PUSH_SYNC is gb_pagerank_push. */
+#define GB_PR_PUSH_ASYNC 0
+#define GB_PR_PUSH_SYNC 1
+int gb_pagerank_push_ex(gb_graph* g, int algo, float alpha, float tol,
+                        uint32_t max_iter, float* rank_out, uint32_t* iters_out,
+                        gb_stats* stats, void* stream);
 /* PageRank pull-residual (PageRank-pull.cpp:132-190): delta/residual rounds
  * over the stored (transposed) graph. */
 int gb_pagerank_pull_residual(gb_graph* g, float alpha, float tol,

@@ -13,7 +13,8 @@ import oracle
 from galois_b200 import assign_weights_u32, rmat, transpose, write_gr
 
 BIN = Path(__file__).resolve().parents[1] / "galois_b200" / "apps" / "bin"
-APPS = ["bfs-gpu", "bfs-directionopt-gpu", "sssp-gpu", "cc-gpu", "pagerank-gpu", "bc-gpu", "operator-example"]
+APPS = ["bfs-gpu", "bfs-directionopt-gpu", "sssp-gpu", "cc-gpu", "pagerank-gpu", "pagerank-push-gpu", "bc-gpu",
+        "operator-example"]
 
 
 def run(app, *args, check=True):
@@ -55,6 +56,11 @@ def test_app_flag_contracts(tmp_path):
     assert p.returncode == 1 and "symmetric" in p.stderr
     p = run("pagerank-gpu", tmp_path / "x.gr", check=False)
     assert p.returncode == 1 and "transposed" in p.stderr
+    # -algo values each app accepts (the pull app's Residual/Topo, the push app's Async/Sync)
+    p = run("pagerank-gpu", tmp_path / "x.gr", "-transposedGraph", "-algo=Async", check=False)
+    assert p.returncode == 1 and "unknown -algo" in p.stderr
+    p = run("pagerank-push-gpu", tmp_path / "x.gr", "-algo=Topo", check=False)
+    assert p.returncode == 1 and "unknown -algo" in p.stderr
 
 
 # ---- GPU --------------------------------------------------------------------------
@@ -141,13 +147,32 @@ def test_cc_gpu_app(cuda_device, graphs, algo, reorder):
 @pytest.mark.gpu
 def test_pagerank_gpu_app(cuda_device, graphs):
     d, _, gt, _ = graphs
-    p = run("pagerank-gpu", d / "gt.gr", "-transposedGraph", "-tolerance=1e-6")
+    p = run("pagerank-gpu", d / "gt.gr", "-transposedGraph", "-tolerance=1e-6", "-algo=Topo")
     want, _ = oracle.pr_pull_topo_f64(gt, 0.85, 1e-6, 1000)
     top = [ln.split() for ln in p.stdout.split("Rank PageRank Id\n")[1].splitlines()[:5]]
     for _, val, vid in top:
         assert abs(float(val) - want[int(vid)]) <= 1e-5
     assert int(top[0][2]) == int(np.argmax(want))
     assert stats(p.stdout)[("PageRank", "Iterations")] >= 1
+
+
+@pytest.mark.gpu
+def test_pagerank_apps_default_algorithms(cuda_device, graphs):
+    """The defaults of the reference apps: pull runs Residual
+    (PageRank-pull.cpp:34-37), push runs Async (PageRank-push.cpp:42-47).
+    At tolerance 1e-7 both list the top vertices of the FP64 fixed point
+    x = (1 - alpha) + alpha * sum x[u] / nout[u] within 1e-5 relative."""
+    d, _, gt, _ = graphs
+    xstar, _ = oracle.pr_pull_topo_f64(gt, 0.85, 1e-15, 5000)
+    xstar *= gt.n
+    for app, args, algo in (("pagerank-gpu", ["-transposedGraph"], "Residual"), ("pagerank-push-gpu", [], "Async")):
+        # the push app reads the graph itself: on this symmetric graph, the same file
+        p = run(app, d / "gt.gr", *args, "-tolerance=1e-7")
+        assert f"Running {algo} version" in p.stdout, p.stdout
+        top = [ln.split() for ln in p.stdout.split("Rank PageRank Id\n")[1].splitlines()[:5]]
+        for _, val, vid in top:
+            want = xstar[int(vid)]
+            assert abs(float(val) - want) <= 1e-5 * max(1.0, want), (app, vid)
 
 
 @pytest.mark.gpu

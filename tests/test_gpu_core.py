@@ -316,14 +316,49 @@ def test_pagerank_residual_vs_restatement(cuda_device, name, method, restated, s
     assert abs(st["iterations"] - it64) <= 2, f"{name}: {st['iterations']} rounds vs {it64}"
 
 
-@pytest.mark.parametrize("name,method,restated", RESIDUAL)
-def test_pagerank_residual_converges_to_fixed_point(cuda_device, name, method, restated):
-    """At tolerance 1e-9 the residual variants reach the PageRank fixed point
+@pytest.mark.parametrize("method,kw", [("pagerank_pull_residual", {}), ("pagerank_push", {}),
+                                       ("pagerank_push", {"algo": "async"})])
+def test_pagerank_residual_converges_to_fixed_point(cuda_device, method, kw):
+    """At tolerance 1e-9 the residual variants -- pull-residual, push Sync and
+    push Async (PageRank-push.cpp:68-101, whose schedule no serial
+    restatement fixes) -- reach the PageRank fixed point
     x = (1 - alpha) + alpha * sum x[u] / nout[u] (the FP64 Jacobi solution
     scaled by n) within 1e-5 relative per vertex (absolute below 1)."""
     g, _ = rmat(14, 16, seed=41)
     xstar, _ = oracle.pr_pull_topo_f64(g, 0.85, 1e-15, 5000)
     xstar *= g.n
     with DeviceGraph(g, symmetric=True) as dg:
-        got = getattr(dg, method)(0.85, 1e-9, 1000)
-    assert _rel(got, xstar) <= 1e-5, name
+        got = getattr(dg, method)(0.85, 1e-9, 1000, **kw)
+    assert _rel(got, xstar) <= 1e-5, (method, kw)
+
+
+def test_pagerank_push_async_app_tolerance_and_shapes(cuda_device):
+    """Async push at the app's default tolerance 1e-3: every vertex ends
+    within the leftover-residual bound of the fixed point (below 1e-2
+    relative on these graphs; the Sync restatement at the same tolerance is
+    as far), on a graph with hubs split into tiles, a directed graph with
+    dangling vertices, and a path."""
+    g, _ = rmat(13, 16, seed=23)
+    xstar, _ = oracle.pr_pull_topo_f64(g, 0.85, 1e-15, 5000)
+    xstar *= g.n
+    want_sync, _ = oracle.pr_push_sync(g, 0.85, 1e-3, 1000)
+    with DeviceGraph(g, symmetric=True) as dg:
+        dg.set_tuning(heavy_degree=32, tile_edges=64)
+        got, st = dg.pagerank_push(0.85, 1e-3, 1000, stats=True, algo="async")
+    assert st["iterations"] == 1
+    assert _rel(got, xstar) <= 1e-2 and _rel(want_sync, xstar) <= 1e-2
+    # a directed graph: the push goes along out-arcs; its fixed point is the
+    # transposed graph's pull solution
+    gd, _ = rmat(11, 8, seed=4, symmetrize=False)
+    from galois_b200 import transpose
+
+    gt, _ = transpose(gd)
+    xd, _ = oracle.pr_pull_topo_f64(gt, 0.85, 1e-15, 5000)
+    xd *= gd.n
+    with DeviceGraph(gd, symmetric=False) as dg:
+        got = dg.pagerank_push(0.85, 1e-9, 1000, algo="async")
+    assert _rel(got, xd) <= 1e-5
+    with DeviceGraph(path_graph(500), symmetric=True) as dg:
+        got = dg.pagerank_push(0.85, 1e-9, 1000, algo="async")
+    xp, _ = oracle.pr_pull_topo_f64(path_graph(500), 0.85, 1e-15, 5000)
+    assert _rel(got, xp * 500) <= 1e-5
