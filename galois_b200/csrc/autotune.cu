@@ -117,10 +117,10 @@ extern "C" int gb_autotune(gb_graph* g, const char* kernel, uint32_t src, const 
       if (k == "sssp") {
         for (int depth : {-1, 2, 8, 16}) {
           t.local_depth = depth;
-          t.sssp_async = -1;
+          t.sssp_async = 0;
           cands.push_back(t);
           if (depth > 0) {  // asynchronous buckets (taken only when every vertex is light)
-            t.sssp_async = 0;
+            t.sssp_async = 1;
             cands.push_back(t);
           }
         }

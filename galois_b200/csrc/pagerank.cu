@@ -91,7 +91,7 @@ struct PrArgs {
   uint32_t* stamp;
   FrontierQueues fq;
   uint32_t heavy, tile;
-  wl::Ring ring;  // Async push: the worklist ring
+  worklists::Ring ring;  // Async push: the worklist ring
   uint32_t zero_from;  // first vertex of the no-in-arc suffix (degree-ordered graphs), else n
   // flat sweep of the light rows (degree-ordered graphs): arcs [lr_arc0,
   // lr_arc1) in runs of kLightRun; an arc's row is lr_runrow[run] +
@@ -667,7 +667,7 @@ __global__ void __launch_bounds__(kBlock, 1) pr_push_async(PrArgs a) {
   const uint64_t deadline = kernel_deadline();
   const uint32_t lane = lane_id();
   unsigned long long my_push = 0, my_absorb = 0;
-  wl::WarpQueue<kPushLQ> q(s_lq[threadIdx.x >> 5], a.ring, &ctl->err, deadline);
+  worklists::WarpQueue<kPushLQ> q(s_lq[threadIdx.x >> 5], a.ring, &ctl->err, deadline);
   const float tol = a.tol;
   // add d to u's residual; activate u when the add lifts it across tol
   // (old < tol <= old + d, PageRank-push.cpp:92-94)
@@ -776,11 +776,11 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
   // Async: the initial worklist (every vertex, 32 per chunk) plus room for
   // as many chunks again and the tiles of the heavy vertices
   const uint32_t nchunks = (uint32_t)(((uint64_t)n + 31) / 32);
-  const unsigned long long cap = wl::ring_capacity(2ull * nchunks + g->m / ((uint64_t)t.tile_edges * 32) + 8192);
+  const unsigned long long cap = worklists::ring_capacity(2ull * nchunks + g->m / ((uint64_t)t.tile_edges * 32) + 8192);
   size_t need = carve_size<PrCtl>(1) + 5 * carve_size<float>(n) + (out_dev ? 0 : carve_size<float>(n));
   if (kind != PrKind::Pull) need += 2 * carve_size<float>(n);
   if (kind == PrKind::Push) need += 3 * carve_size<uint32_t>(n) + fl.bytes;
-  if (kind == PrKind::PushAsync) need += carve_size<char>(wl::ring_bytes(cap));
+  if (kind == PrKind::PushAsync) need += carve_size<char>(worklists::ring_bytes(cap));
   st = ws_reserve(g, need, s);
   if (st != GB_OK) return st;
   Carver cv(g->ws);
@@ -800,7 +800,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
     a.stamp = cv.take<uint32_t>(n);
     a.fq = carve_frontier(cv, fl);
   }
-  if (kind == PrKind::PushAsync) a.ring = wl::ring_layout(cv.take<char>(wl::ring_bytes(cap)), cap);
+  if (kind == PrKind::PushAsync) a.ring = worklists::ring_layout(cv.take<char>(worklists::ring_bytes(cap)), cap);
   a.value = out_dev ? rank_out : cv.take<float>(n);
   a.offs = g->offs;
   a.col = g->col;
@@ -864,7 +864,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
     pr_push_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     kfn = reinterpret_cast<const void*>(&pr_push_persistent);
   } else {
-    GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(wl::RingCtl), s));
+    GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(worklists::RingCtl), s));
     pr_push_async_init<<<g->sm_count * 4, 256, 0, s>>>(a, nchunks);
     kfn = reinterpret_cast<const void*>(&pr_push_async);
   }

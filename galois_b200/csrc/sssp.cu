@@ -41,21 +41,22 @@
 // separated by the bounded grid barrier.
 
 //
-// Bounded-degree graphs (every vertex light and the local queues on: grids,
-// road-like graphs) run an asynchronous form instead (sssp_async below): the
-// phases of a bucket are not separated by grid barriers at all.  Each warp
-// keeps relaxing its own local queue; improvements that do not fit, and a
-// warp's surplus while other warps wait for work, are published as chunks of
-// up to 32 entries in a ring; a warp without work takes the next ring
-// position (a ticket) and waits for its chunk.  A bucket ends when a single
-// counter -- busy warps plus published, unconsumed chunks -- reaches zero;
-// only the bucket transitions keep grid barriers.  On such graphs a bucket's
-// shortest-path chains are hundreds of hops long and the phase barrier, not
-// the relaxations, set the time.
+// sssp_async (tuning sssp_async > 0) is an alternative schedule for
+// bounded-degree graphs (every vertex light, local queues on): no grid
+// barrier between the phases of a bucket; each warp keeps relaxing its own
+// local queue and shares surplus through the device worklist
+// (gb_worklist.cuh); a bucket ends when the worklist's work count reaches
+// zero, and only the bucket transitions keep grid barriers -- the schedule
+// of the reference's barrier-free OBIM inside a bucket.  On the 4096^2 grid
+// it measured 42.5-44 ms against 40.8 ms for the phase-synchronous kernel
+// (more arcs re-relaxed, 9.7x against 6.7x the reached arcs, while the
+// ~8 K-hop dependent chain sets both times), so the phase-synchronous
+// kernel stays the default.
 
 #include "device_common.cuh"
 #include "device_graph.cuh"
 #include "frontier.cuh"
+#include "gb_worklist.cuh"
 #include "sweep.cuh"
 
 namespace gb {
@@ -88,30 +89,6 @@ struct SsspCtl {
   unsigned long long relax;
 };
 
-// Control words of the chunk ring of sssp_async, each on its own 128-byte line
-// (every waiting warp polls them).
-struct alignas(128) RingCtl {
-  unsigned long long head;  // ring positions taken by warps waiting for work (tickets)
-  unsigned long long pad0[15];
-  unsigned long long tail;  // ring positions published
-  unsigned long long pad1[15];
-  int work;  // busy warps + published chunks not yet taken: 0 ends the bucket
-  int pad2[31];
-  unsigned long long chunks;  // chunks published (statistics)
-  unsigned long long pad3[15];
-};
-
-// The chunk ring: position p lives in slot p & mask.  seq[slot] == p: free for
-// the producer of position p; == p + 1: published, for the consumer of p;
-// the consumer sets it to p + cap, freeing the slot for the next lap.
-struct ChunkRing {
-  uint4* ent;               // [cap][32] entries (vertex, dist, begin lo, begin hi << 16 | degree)
-  unsigned long long* seq;  // [cap]
-  uint32_t* cnt;            // [cap] entries in the chunk
-  unsigned long long mask;  // cap - 1 (cap a power of two)
-  RingCtl* rc;
-};
-
 struct SsspArgs {
   const uint64_t* __restrict__ offs;
   const uint32_t* __restrict__ col;
@@ -134,7 +111,7 @@ struct SsspArgs {
   const uint2* sw_tiles;  // cached (vertex, k) tiles of every heavy vertex
   uint32_t sw_ntiles;
   uint32_t bm_min;  // frontier estimate above which the next frontier is a bitmap
-  ChunkRing ring;   // sssp_async only
+  worklists::Ring ring;  // sssp_async only
 };
 
 __global__ void sssp_init(SsspArgs a) {
@@ -536,85 +513,7 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(SsspArgs a) {
 
 // ---- asynchronous buckets (bounded-degree graphs) ----------------------------
 
-constexpr int kAsyncLQ = 64;                          // local-queue entries per warp
-constexpr uint64_t kRingSlotWaitNs = 2000000000ull;   // a producer's wait for a free slot
-
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
-  return *reinterpret_cast<const volatile unsigned long long*>(p);
-}
-
-// Publish the entries of the lanes with `pred` as one chunk (warp-collective).
-// The chunk is counted in `work` before it becomes visible, while this warp
-// is itself busy, so the count never reads zero with work outstanding.
-// Returns false when the slot stayed occupied past the wait limit (the ring
-// is full; the error word is raised) or another warp raised an error.
-__device__ __forceinline__ bool ring_publish(const ChunkRing& r, bool pred, uint4 e, int* err) {
-  const unsigned m = __ballot_sync(kFull, pred);
-  if (!m) return true;
-  const uint32_t lane = lane_id();
-  unsigned long long p = 0;
-  int ok = 1;
-  if (lane == 0) {
-    atomicAdd(&r.rc->work, 1);
-    p = atomicAdd(&r.rc->tail, 1ull);
-    atomicAdd(&r.rc->chunks, 1ull);
-    // the slot is free once the consumer of the previous lap released it
-    const unsigned long long* sq = r.seq + (p & r.mask);
-    uint64_t t0 = 0;
-    unsigned spins = 0;
-    while (ld_acquire_u64(sq) != p) {
-      if ((++spins & 63u) == 0) {
-        const uint64_t now = globaltimer_ns();
-        if (!t0) t0 = now;
-        if (read_err(err)) { ok = 0; break; }
-        if (now - t0 > kRingSlotWaitNs) { raise_err(err, kDevOverflow); ok = 0; break; }
-      }
-      __nanosleep(64);
-    }
-  }
-  p = __shfl_sync(kFull, p, 0);
-  ok = __shfl_sync(kFull, ok, 0);
-  if (!ok) return false;
-  const unsigned long long slot = p & r.mask;
-  if (pred) r.ent[slot * 32 + __popc(m & ((1u << lane) - 1u))] = e;
-  if (lane == 0) r.cnt[slot] = (uint32_t)__popc(m);
-  __syncwarp();
-  if (lane == 0) {
-    __threadfence();
-    st_release_u64(r.seq + slot, p + 1);
-  }
-  return true;
-}
-
-// Lane 0 of a warp without work: wait for the chunk of ring position p.
-// 1: published; 0: the bucket has no work left anywhere; -1: an error was
-// raised or the kernel passed its deadline (kDevTimeout raised).
-__device__ __forceinline__ int ring_wait(const ChunkRing& r, unsigned long long p, int* err, uint64_t deadline) {
-  const unsigned long long* sq = r.seq + (p & r.mask);
-  unsigned spins = 0, ns = 32;
-  for (;;) {
-    if (ld_acquire_u64(sq) == p + 1) return 1;
-    if ((++spins & 7u) == 0) {
-      // work counts every busy warp and every published chunk, ours included
-      if (*reinterpret_cast<const volatile int*>(&r.rc->work) == 0) return 0;
-      if (read_err(err)) return -1;
-      if (globaltimer_ns() > deadline) {
-        raise_err(err, kDevTimeout);
-        return -1;
-      }
-    }
-    __nanosleep(ns);
-    if (ns < 512) ns <<= 1;
-  }
-}
+constexpr int kAsyncLQ = 64;  // local-queue entries per warp
 
 __global__ void sssp_async_init(SsspArgs a) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -637,42 +536,21 @@ __global__ void sssp_async_init(SsspArgs a) {
   }
 }
 
-// Bitonic sort of one 64-bit value per lane across the warp (ascending or
-// descending by lane).
-__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v, bool ascending) {
-  const uint32_t lane = lane_id();
-#pragma unroll
-  for (uint32_t k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-      const unsigned long long o = __shfl_xor_sync(kFull, v, j);
-      // the k-block runs up (ascending) or down; its lower lane of each pair
-      // keeps the minimum when the block runs up
-      const bool up = ((lane & k) == 0) == ascending;
-      const bool take_min = ((lane & j) == 0) == up;
-      v = take_min ? (o < v ? o : v) : (o > v ? o : v);
-    }
-  }
-  return v;
-}
-
 // Delta-stepping with asynchronous buckets.  Needs every vertex light
-// (degree <= a.heavy, < 65536) and offsets below 2^48 (entries pack them).
-// kMode bit 0: prefetch the arcs of every vertex queued (into L2) while its
-// entry waits; bit 1: a round takes the 32 queued entries of smallest
-// distance instead of the 32 most recent.
-template <int BLOCK, int kMode>
+// (degree <= a.heavy, < 65536) and offsets below 2^48: worklist entries are
+// (vertex, distance, begin offset low, begin offset high << 16 | degree).
+template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) sssp_async(SsspArgs a) {
+  static_assert(worklists::kErrTimeout == kDevTimeout && worklists::kErrOverflow == kDevOverflow,
+                "the worklist raises the library's device error codes");
   __shared__ uint4 s_lq[BLOCK / 32][kAsyncLQ];
   SsspCtl* ctl = a.ctl;
-  RingCtl* rc = a.ring.rc;
+  worklists::RingCtl* rc = a.ring.rc;
   const unsigned nblocks = gridDim.x;
   const uint64_t deadline = kernel_deadline();
   const uint32_t lane = lane_id();
   const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
   const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
-  const unsigned lanemask_lt = (1u << lane) - 1u;
-  uint4* lq = s_lq[threadIdx.x >> 5];
   unsigned long long my_scanned = 0, my_relax = 0;
 
   uint32_t bucket = 0;
@@ -687,11 +565,10 @@ __global__ void __launch_bounds__(BLOCK) sssp_async(SsspArgs a) {
     const uint32_t hi = hi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)hi64;
     uint32_t* farq = a.far[fp];
     // ---- the bucket's work, no grid barrier --------------------------------
-    uint32_t lq_n = 0;   // warp-uniform local queue length
-    bool busy = false;   // this warp holds one count of rc->work
-    // Relax arc (v -> u) to nd: near improvements go to the local queue, the
-    // ones that do not fit to the ring; far ones to the far pile (once, by
-    // the bitmap).  The target's offsets load beside the atomic.
+    worklists::WarpQueue<kAsyncLQ> q(s_lq[threadIdx.x >> 5], a.ring, &ctl->err, deadline);
+    // Relax to nd the arc into u: near improvements join the worklist, far
+    // ones the far pile (once, by the bitmap).  The target's offsets load
+    // beside the atomic.
     auto relax = [&](bool valid, uint32_t u, uint32_t nd) {
       bool near = false, far = false;
       uint64_t ub = 0, deg = 0;
@@ -709,73 +586,16 @@ __global__ void __launch_bounds__(BLOCK) sssp_async(SsspArgs a) {
           }
         }
       }
-      const unsigned nm = __ballot_sync(kFull, near);
-      if (nm) {
-        const uint32_t k = __popc(nm), room = kAsyncLQ - lq_n, rank = __popc(nm & lanemask_lt);
-        const uint4 e = make_uint4(u, nd, (uint32_t)ub, (uint32_t)((ub >> 32) << 16) | (uint32_t)deg);
-        const bool loc = near && rank < room;
-        if (loc) lq[lq_n + rank] = e;
-        lq_n += min(k, room);
-        __syncwarp();
-        if (k > room) ring_publish(a.ring, near && !loc, e, &ctl->err);
-        if ((kMode & 1) && near) {
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(a.col + ub));
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(a.w + ub));
-        }
-      }
+      q.push(near, make_uint4(u, nd, (uint32_t)ub, (uint32_t)((ub >> 32) << 16) | (uint32_t)deg));
       warp_push(far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
     };
     for (;;) {
-      uint4 ent = make_uint4(0u, 0u, 0u, 0u);
-      bool has = false;
-      if ((kMode & 2) && lq_n > 32) {
-        // the 32 entries of smallest distance: sort the first 32 up and the
-        // rest down; the lane-wise minima are the 32 smallest of all
-        const bool hb = lane + 32 < lq_n;
-        const unsigned long long ka = ((unsigned long long)lq[lane].y << 32) | lane;
-        const unsigned long long kb = hb ? ((unsigned long long)lq[lane + 32].y << 32) | (lane + 32) : ~0ull;
-        const unsigned long long sa = warp_sort32(ka, true), sb = warp_sort32(kb, false);
-        const unsigned long long mine = sa < sb ? sa : sb, rest = sa < sb ? sb : sa;
-        ent = lq[(uint32_t)mine & 63u];
-        has = true;
-        const bool keep = rest != ~0ull;
-        const uint4 kept = keep ? lq[(uint32_t)rest & 63u] : make_uint4(0u, 0u, 0u, 0u);
-        __syncwarp();
-        const unsigned km = __ballot_sync(kFull, keep);
-        if (keep) lq[__popc(km & lanemask_lt)] = kept;
-        __syncwarp();
-        lq_n -= 32;
-      } else if (lq_n > 0) {
-        const uint32_t take = min(32u, lq_n);
-        has = lane < take;
-        if (has) ent = lq[lq_n - take + lane];
-        __syncwarp();
-        lq_n -= take;
-      } else {
-        // out of work: give up this warp's count, take a ticket, wait for its chunk
-        if (busy && lane == 0) atomicSub(&rc->work, 1);
-        busy = false;
-        unsigned long long p = 0;
-        int got = 0;
-        if (lane == 0) {
-          p = atomicAdd(&rc->head, 1ull);
-          got = ring_wait(a.ring, p, &ctl->err, deadline);
-        }
-        got = __shfl_sync(kFull, got, 0);
-        if (got <= 0) break;  // the bucket is done (or an error was raised)
-        p = __shfl_sync(kFull, p, 0);
-        __syncwarp();  // lane 0's acquire orders the other lanes' reads below
-        busy = true;   // the chunk's count is now this warp's
-        const unsigned long long slot = p & a.ring.mask;
-        const uint32_t c = __ldcg(a.ring.cnt + slot);
-        has = lane < c;
-        if (has) ent = __ldcg(a.ring.ent + slot * 32 + lane);
-        __syncwarp();
-        if (lane == 0) st_release_u64(a.ring.seq + slot, p + a.ring.mask + 1);  // free for the next lap
-      }
+      uint4 ent;
+      bool has;
+      if (q.next(ent, has) <= 0) break;  // the bucket is done (or an error was raised)
       // one round: every lane's vertex, its arcs spread over the warp; an
       // entry whose vertex has a smaller distance by now is stale (whoever
-      // lowered it routed the vertex again)
+      // lowered it queued the vertex again)
       const uint64_t b = ((uint64_t)(ent.w >> 16) << 32) | ent.z;
       const uint32_t d = has ? (ent.w & 0xFFFFu) : 0u;
       const uint32_t cur = has ? __ldcg(a.dist + ent.x) : 0u;
@@ -787,19 +607,7 @@ __global__ void __launch_bounds__(BLOCK) sssp_async(SsspArgs a) {
             const bool live = __shfl_sync(kFull, cur, owner) >= dsrc;
             relax(valid && live, u, nd);
           });
-      // while other warps wait for work, hand them this warp's oldest entries
-      if (lq_n > 32) {
-        int want = 0;
-        if (lane == 0) want = ld_volatile_u64(&rc->head) > ld_volatile_u64(&rc->tail);
-        if (__shfl_sync(kFull, want, 0)) {
-          const uint4 e = lq[lane];
-          __syncwarp();
-          for (uint32_t i = 32 + lane; i < lq_n; i += 32) lq[i - 32] = lq[i];
-          __syncwarp();
-          lq_n -= 32;
-          ring_publish(a.ring, true, e, &ctl->err);
-        }
-      }
+      q.share();
     }
     if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
     // ---- bucket transition ---------------------------------------------------
@@ -848,8 +656,8 @@ __global__ void __launch_bounds__(BLOCK) sssp_async(SsspArgs a) {
           }
           if (!keep) atomicAnd(&a.infar[u >> 5], ~(1u << (u & 31)));
         }
-        ring_publish(a.ring, to_near, make_uint4(u, dd, (uint32_t)ub, (uint32_t)((ub >> 32) << 16) | (uint32_t)deg),
-                     &ctl->err);
+        worklists::publish(a.ring, to_near,
+                           make_uint4(u, dd, (uint32_t)ub, (uint32_t)((ub >> 32) << 16) | (uint32_t)deg), &ctl->err);
         warp_push(keep, u, keepq, &ctl->far_count[fp ^ 1], a.n, &ctl->err);
       }
     }
@@ -932,9 +740,9 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   const uint32_t words = (n + 31) / 32;
   const bool out_dev = is_device_ptr(dist_out);
   const int local_depth = t.local_depth < 0 ? 0 : t.local_depth;
-  // asynchronous buckets: local queues on and every vertex light (entries
-  // pack the degree in 16 bits and the begin offset in 48)
-  const bool async = t.sssp_async >= 0 && local_depth > 0 && g->max_degree <= t.heavy_degree &&
+  // asynchronous buckets (asked for): local queues on and every vertex
+  // light (entries pack the degree in 16 bits and the begin offset in 48)
+  const bool async = t.sssp_async > 0 && local_depth > 0 && g->max_degree <= t.heavy_degree &&
                      g->max_degree < 65536 && g->m < (1ull << 48);
   FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
   SweepSched sched{};
@@ -942,15 +750,12 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
     int sst = ensure_sweep_schedule(g, t.heavy_degree, t.tile_edges, s, &sched);
     if (sst != GB_OK) return sst;
   }
-  // ring of chunks: at least n/32 + 8192 positions (a bucket's split fills at
-  // most one chunk per 32 far entries), a power of two
-  uint64_t cap = 1;
-  while (cap < (uint64_t)n / 32 + 8192) cap <<= 1;
+  // worklist ring: a bucket's split fills at most one chunk per 32 far
+  // entries, the warps' overflow only full chunks
+  const unsigned long long cap = worklists::ring_capacity((uint64_t)n / 16 + 8192);
   size_t need = carve_size<SsspCtl>(1) + carve_size<uint32_t>(words) + 2 * carve_size<uint32_t>(n) +
                 (out_dev ? 0 : carve_size<uint32_t>(n)) + carve_size<unsigned long long>(2);
-  if (async)
-    need += carve_size<RingCtl>(1) + carve_size<uint4>(cap * 32) + carve_size<unsigned long long>(cap) +
-            carve_size<uint32_t>(cap);
+  if (async) need += carve_size<char>(worklists::ring_bytes(cap));
   else
     need += carve_size<uint32_t>(n) + 3 * carve_size<uint32_t>(words) + fl.bytes;
   int st = ws_reserve(g, need, s);
@@ -964,11 +769,7 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   unsigned long long* reach = cv.take<unsigned long long>(2);
   a.dist = out_dev ? dist_out : cv.take<uint32_t>(n);
   if (async) {
-    a.ring.rc = cv.take<RingCtl>(1);
-    a.ring.ent = cv.take<uint4>(cap * 32);
-    a.ring.seq = cv.take<unsigned long long>(cap);
-    a.ring.cnt = cv.take<uint32_t>(cap);
-    a.ring.mask = cap - 1;
+    a.ring = worklists::ring_layout(cv.take<char>(worklists::ring_bytes(cap)), cap);
   } else {
     a.stamp = cv.take<uint32_t>(n);
     for (int i = 0; i < 3; ++i) a.act[i] = cv.take<uint32_t>(words);
@@ -994,15 +795,10 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   a.bm_min = n >> 8;
   if (async) {
     GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), s));
-    GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(RingCtl), s));
+    GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(worklists::RingCtl), s));
     sssp_async_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     GB_CUDA(cudaGetLastError());
-    // sssp_async: 0 = library default, 1..4 = kernel variants 0..3 (prefetch, distance order)
-    const int mode = t.sssp_async == 0 ? 3 : (t.sssp_async - 1) & 3;
-    const void* kfn = mode == 0   ? reinterpret_cast<const void*>(&sssp_async<256, 0>)
-                      : mode == 1 ? reinterpret_cast<const void*>(&sssp_async<256, 1>)
-                      : mode == 2 ? reinterpret_cast<const void*>(&sssp_async<256, 2>)
-                                  : reinterpret_cast<const void*>(&sssp_async<256, 3>);
+    const void* kfn = reinterpret_cast<const void*>(&sssp_async<256>);
     const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
     if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
     void* args[] = {&a};

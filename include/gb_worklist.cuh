@@ -35,7 +35,7 @@
 #include <stdint.h>
 
 namespace gb {
-namespace wl {
+namespace worklists {
 
 // Error codes written into the caller's error word (the library kernels use
 // the same values for their own device errors).
@@ -203,7 +203,7 @@ __device__ __forceinline__ int wait_chunk(const Ring& r, unsigned long long p, i
 // converged); `n` and `busy` are warp-uniform.
 template <int LQ>
 struct WarpQueue {
-  static_assert(LQ >= 32, "the local queue holds at least one round");
+  static_assert(LQ >= 64, "a full local queue holds at least the 32 entries it spills");
   uint4* lq;
   uint32_t n;
   bool busy;
@@ -251,30 +251,24 @@ struct WarpQueue {
     return 1;
   }
 
-  // Append the entries of the lanes with `pred`: to the local queue while it
-  // has room, the rest as one chunk of the ring.
+  // Append the entries of the lanes with `pred` to the local queue.  When
+  // they do not fit, the 32 oldest local entries first leave as one full
+  // chunk of the ring (so overflow never publishes a part-filled chunk, and
+  // the ring holds at most one chunk per 32 entries in flight).
   __device__ void push(bool pred, uint4 e) {
     const unsigned m = __ballot_sync(0xFFFFFFFFu, pred);
     if (!m) return;
     const unsigned lane = threadIdx.x & 31u;
-    const uint32_t k = __popc(m), room = LQ - n, rank = __popc(m & ((1u << lane) - 1u));
-    const bool loc = pred && rank < room;
-    if (loc) lq[n + rank] = e;
-    n += k < room ? k : room;
+    const uint32_t k = __popc(m);
+    if (n + k > (uint32_t)LQ) spill_oldest();
+    if (pred) lq[n + __popc(m & ((1u << lane) - 1u))] = e;
+    n += k;
     __syncwarp();
-    if (k > room) publish(ring, pred && !loc, e, err);
   }
 
-  // While other warps wait for work (tickets beyond the published tail),
-  // hand them this warp's 32 oldest local entries.
-  __device__ void share() {
-    if (n <= 32) return;
+  // Publish the 32 oldest local entries as one chunk (n >= 32).
+  __device__ void spill_oldest() {
     const unsigned lane = threadIdx.x & 31u;
-    int want = 0;
-    if (lane == 0)
-      want = *reinterpret_cast<const volatile unsigned long long*>(&ring.rc->head) >
-             *reinterpret_cast<const volatile unsigned long long*>(&ring.rc->tail);
-    if (!__shfl_sync(0xFFFFFFFFu, want, 0)) return;
     const uint4 e = lq[lane];
     __syncwarp();
     for (uint32_t i = 32 + lane; i < n; i += 32) lq[i - 32] = lq[i];
@@ -282,7 +276,18 @@ struct WarpQueue {
     n -= 32;
     publish(ring, true, e, err);
   }
+
+  // While other warps wait for work (tickets beyond the published tail),
+  // hand them this warp's 32 oldest local entries.
+  __device__ void share() {
+    if (n <= 32) return;
+    int want = 0;
+    if ((threadIdx.x & 31u) == 0)
+      want = *reinterpret_cast<const volatile unsigned long long*>(&ring.rc->head) >
+             *reinterpret_cast<const volatile unsigned long long*>(&ring.rc->tail);
+    if (__shfl_sync(0xFFFFFFFFu, want, 0)) spill_oldest();
+  }
 };
 
-}  // namespace wl
+}  // namespace worklists
 }  // namespace gb

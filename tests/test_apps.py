@@ -193,7 +193,26 @@ def test_bc_gpu_app(cuda_device, graphs, tmp_path):
 
 
 @pytest.mark.gpu
-def test_operator_example(cuda_device, graphs):
-    d, _, _, src = graphs
-    p = run("operator-example", d / "g.gr", f"-startNode={src}")
-    assert "0 mismatches" in p.stdout and "Verification successful." in p.stdout
+@pytest.mark.parametrize("delta", [13, 4])
+def test_operator_example(cuda_device, graphs, tmp_path, delta):
+    """The operator layer (gb::for_each_edge with gb::wl<gb::FIFO>() for the
+    asynchronous BFS operator and gb::wl<gb::DeltaBuckets>(delta) for the
+    SSSP operator of SSSP.cpp:134-161) against the oracle, bit-exact: the
+    RMAT graph of the other app tests, and a star of 5000 leaves (its hub's
+    arcs run as 1024-arc tiles) joined to a path."""
+    from galois_b200 import HostCSR
+
+    d, g, _, src = graphs
+    k = 5000
+    s_ = [0] * k + list(range(1, k + 1)) + list(range(k, k + 99)) + list(range(k + 1, k + 100))
+    t_ = list(range(1, k + 1)) + [0] * k + list(range(k + 1, k + 100)) + list(range(k, k + 99))
+    star = HostCSR.from_edges(k + 100, s_, t_)
+    star = assign_weights_u32(star, 1, 255, seed=9)
+    write_gr(str(tmp_path / "star.gr"), star, 4)
+    for path, gg, source in ((d / "g.gr", g, src), (tmp_path / "star.gr", star, 0), (tmp_path / "star.gr", star, k + 50)):
+        out = tmp_path / "res.bin"
+        p = run("operator-example", path, f"-startNode={source}", f"-delta={delta}", f"-output={out}")
+        assert "Verification successful." in p.stdout
+        res = np.fromfile(out, dtype=np.uint32)
+        assert np.array_equal(res[:gg.n], oracle.bfs_serial(gg, source)), path
+        assert np.array_equal(res[gg.n:], oracle.sssp_dijkstra(gg, source)), path

@@ -180,11 +180,11 @@ def test_sssp_async_buckets_bit_exact(cuda_device, shift):
         with DeviceGraph(g, symmetric=True) as dg:
             for src in srcs:
                 want = oracle.sssp_dijkstra(g, src)
-                dg.set_tuning(local_depth=8, sssp_async=0)
+                dg.set_tuning(local_depth=8, sssp_async=1)
                 got, st = dg.sssp(src, shift, stats=True)
                 assert (got == want).all(), f"async n={g.n} src={src}"
                 assert st["vertices_reached"] == int((want != INF).sum())
-                dg.set_tuning(sssp_async=-1)
+                dg.set_tuning(sssp_async=0)
                 assert (dg.sssp(src, shift) == want).all(), f"phase-synchronous n={g.n} src={src}"
 
 
@@ -195,11 +195,12 @@ def test_sssp_async_small_ring_and_blocks(cuda_device):
     assign_weights_u32(g, 1, 255, seed=77)
     want = oracle.sssp_dijkstra(g, 777)
     with DeviceGraph(g, symmetric=True) as dg:
-        dg.set_tuning(local_depth=4, blocks_per_sm=1)
+        dg.set_tuning(local_depth=4, blocks_per_sm=1, sssp_async=1)
         assert (dg.sssp(777, 13) == want).all()
     iso = union(path_graph(1), grid2d(10, 10))
     iso.w_u32 = np.ones(iso.m, np.uint32)
     with DeviceGraph(iso, symmetric=True) as dg:
+        dg.set_tuning(sssp_async=1)
         got = dg.sssp(0, 13)
         assert got[0] == 0 and (got[1:] == INF).all()
 
