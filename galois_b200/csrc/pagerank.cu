@@ -332,6 +332,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
   const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
   const uint32_t lane = lane_id();
   constexpr int UT = 8;
+  // the column ids and row offsets stream through once per sweep; the
+  // contributions they gather should stay in L2
+  const uint64_t stream = l2_policy_evict_first(), keep = l2_policy_evict_last();
   const uint64_t nruns = (a.lr_arc1 - a.lr_arc0 + 32 * UT - 1) / (32 * UT);
   const uint64_t total = (uint64_t)a.sched.ntiles + nruns;
   for (uint32_t it = 0;; ++it) {
@@ -351,7 +354,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
 #pragma unroll
         for (int k = 0; k < UT; ++k) {
           const uint64_t i = b + lane + 32 * k;
-          u[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
+          u[k] = i < e ? ld_stream(a.col + i, stream) : 0xFFFFFFFFu;
         }
         float sum = 0.f;
         for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
@@ -359,10 +362,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
 #pragma unroll
           for (int k = 0; k < UT; ++k) {
             const uint64_t i = i0 + 32 * UT + lane + 32 * k;
-            un[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
+            un[k] = i < e ? ld_stream(a.col + i, stream) : 0xFFFFFFFFu;
           }
 #pragma unroll
-          for (int k = 0; k < UT; ++k) sum += u[k] != 0xFFFFFFFFu ? c_in[u[k]] : 0.f;
+          for (int k = 0; k < UT; ++k) sum += u[k] != 0xFFFFFFFFu ? ld_keep_f32(c_in + u[k], keep) : 0.f;
 #pragma unroll
           for (int k = 0; k < UT; ++k) u[k] = un[k];
         }
@@ -379,12 +382,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
         for (int k = 0; k < UT; ++k) {
           const uint64_t i = r0 + lane + 32 * k;
           const bool ok = i < a.lr_arc1;
-          u[k] = ok ? ldg(a.col + i) : 0u;
-          row[k] = ok ? row0 + (uint32_t)__ldg(a.lr_rowd + (i - a.lr_arc0)) : 0xFFFFFFFFu;
+          u[k] = ok ? ld_stream(a.col + i, stream) : 0u;
+          row[k] = ok ? row0 + ld_stream_u8(a.lr_rowd + (i - a.lr_arc0), stream) : 0xFFFFFFFFu;
         }
         float x[UT];
 #pragma unroll
-        for (int k = 0; k < UT; ++k) x[k] = row[k] != 0xFFFFFFFFu ? c_in[u[k]] : 0.f;
+        for (int k = 0; k < UT; ++k) x[k] = row[k] != 0xFFFFFFFFu ? ld_keep_f32(c_in + u[k], keep) : 0.f;
 #pragma unroll
         for (int k = 0; k < UT; ++k) {
           if (seg_reduce(row[k] != 0xFFFFFFFFu, row[k], x[k])) atomicAdd(&acc_cur[row[k]], x[k]);
