@@ -900,8 +900,8 @@ def roofline_of(job: Job, r: dict, order: int, traffic) -> dict:
     need = min(r["bytes_step"], r["work_step"])
     return {"bound": "hbm", "achieved": need / sec / 1e9, "peak": peak, "unit": "GB/s",
             "frac": need / sec / 1e9 / peak, "peak_source": peak_src,
-            # a degree-ordered PageRank runs the flat pull kernel
-            "kernel": "pr_pull_flat" if (type(job) is PrJob and order) else job.kernel,
+            # a degree-ordered PageRank runs the flat pull kernels
+            "kernel": job.kernel.replace("_persistent", "_flat") if (isinstance(job, PrJob) and order) else job.kernel,
             "bytes_counted_per_step": need,
             "algorithmic_bytes_per_step": r["bytes_step"], "kernel_ms_per_step": sum(r["kms"]),
             "model_frac": r["bytes_step"] / sec / 1e9 / peak,
@@ -952,6 +952,58 @@ def run_apps(args, dev: int) -> dict:
                     "cpu_baseline": {"value": cpu_units / t_cpu / 1e9, "unit": job.unit, "cores": oracle.threads(),
                                      "kind": "port", "sample": "one full run of the same workload"}}
     return out
+
+
+def run_ppr_sharded(args) -> None:
+    """--app ppr on N GPUs: the 128 teleport columns are sharded over the
+    ranks (blocks of multiples of 4) and one NCCL all-reduce sums the
+    edge-weight gradient (strong scaling: the total work is fixed)."""
+    import torch
+
+    from galois_b200 import DeviceGraph, assign_weights_f32, rmat
+    from galois_b200.distributed import ppr_sharded
+
+    dist = Dist(want_pg=True)
+    dev = dist.local_rank
+    torch.cuda.set_device(dev)
+    scale = pick(args.size, 16, 19, 22)
+    g, _ = rmat(scale, 16, seed=22, symmetrize=False)
+    assign_weights_f32(g, seed=22)
+    B = 128
+    rng = np.random.default_rng(128)
+    T = torch.zeros((g.n, B), dtype=torch.float32, device=f"cuda:{dev}")
+    for b in range(B):
+        T[torch.from_numpy(rng.choice(g.n, 32, replace=False)).to(T.device), b] = 1.0 / 32
+    c = torch.from_numpy(rng.standard_normal((g.n, B)).astype(np.float32)).to(T.device)
+    dg = DeviceGraph(g, device=dev)
+    w = torch.from_numpy(g.w_f32).to(T.device)
+    for _ in range(max(args.warmup, 1)):
+        ppr_sharded(dg, T, w, c, 0.85, 1e-7)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ppr_sharded(dg, T, w, c, 0.85, 1e-7)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    t_ms = dist.max(e0.elapsed_time(e1))
+    if dist.rank == 0:
+        emit({"metric": "PPR forward+adjoint columns per second (batch 128, tol 1e-7)", "unit": "columns/s",
+              "value": B * args.steps / (t_ms / 1e3), "n_gpus": dist.world, "steps": args.steps,
+              "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+              "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+              "config": {"workload": f"personalised PageRank + adjoint, RMAT-{scale} directed ef16, 128 teleports "
+                                     f"sharded over {dist.world} GPUs in blocks of 4 columns, one all-reduce of "
+                                     "grad_w per step", "n": g.n, "m": g.m, "parallelism": f"columns/{dist.world}"},
+              "clocks": clk, "gpu_launches": 12 * args.steps})
+    dg.free()
+    dist.close()
 
 
 def cpu_units(job: Job, gpu_stats: list) -> float:
@@ -1012,6 +1064,8 @@ def main() -> None:
             return
         if args.app == "bc" and int(os.environ.get("WORLD_SIZE", "1")) > 1:
             run_bc_sharded(args)  # every rank: sources sharded, one all-reduce
+        elif args.app == "ppr" and int(os.environ.get("WORLD_SIZE", "1")) > 1:
+            run_ppr_sharded(args)  # every rank: columns sharded, one all-reduce of grad_w
         elif rank == 0:
             run_batched(args)
         return

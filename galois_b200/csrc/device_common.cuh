@@ -251,37 +251,4 @@ __device__ __forceinline__ void warp_expand_mlp(uint64_t beg, uint32_t deg, uint
 template <class T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
 
-// L2 cache policies for instruction-level eviction hints: a stream read once
-// per sweep (column ids) goes first, the array gathered at random (PageRank
-// contributions) stays, so the stream does not push the gathered array out
-// of L2.
-__device__ __forceinline__ uint64_t l2_policy_evict_first() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ uint64_t l2_policy_evict_last() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-// Read-only stream load: not kept in L1, L2 priority from `pol`.
-__device__ __forceinline__ uint32_t ld_stream(const uint32_t* p, uint64_t pol) {
-  uint32_t v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ uint32_t ld_stream_u8(const uint8_t* p, uint64_t pol) {
-  uint16_t v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u8 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
-  return v;
-}
-// Coherent load (data written earlier in the same launch, ordered by a grid
-// barrier) with an L2 priority.
-__device__ __forceinline__ float ld_keep_f32(const float* p, uint64_t pol) {
-  float v;
-  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
-  return v;
-}
-
 }  // namespace gb

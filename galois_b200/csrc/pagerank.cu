@@ -332,9 +332,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
   const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
   const uint32_t lane = lane_id();
   constexpr int UT = 8;
-  // the column ids and row offsets stream through once per sweep; the
-  // contributions they gather should stay in L2
-  const uint64_t stream = l2_policy_evict_first(), keep = l2_policy_evict_last();
   const uint64_t nruns = (a.lr_arc1 - a.lr_arc0 + 32 * UT - 1) / (32 * UT);
   const uint64_t total = (uint64_t)a.sched.ntiles + nruns;
   for (uint32_t it = 0;; ++it) {
@@ -354,7 +351,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
 #pragma unroll
         for (int k = 0; k < UT; ++k) {
           const uint64_t i = b + lane + 32 * k;
-          u[k] = i < e ? ld_stream(a.col + i, stream) : 0xFFFFFFFFu;
+          u[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
         }
         float sum = 0.f;
         for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
@@ -362,10 +359,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
 #pragma unroll
           for (int k = 0; k < UT; ++k) {
             const uint64_t i = i0 + 32 * UT + lane + 32 * k;
-            un[k] = i < e ? ld_stream(a.col + i, stream) : 0xFFFFFFFFu;
+            un[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
           }
 #pragma unroll
-          for (int k = 0; k < UT; ++k) sum += u[k] != 0xFFFFFFFFu ? ld_keep_f32(c_in + u[k], keep) : 0.f;
+          for (int k = 0; k < UT; ++k) sum += u[k] != 0xFFFFFFFFu ? c_in[u[k]] : 0.f;
 #pragma unroll
           for (int k = 0; k < UT; ++k) u[k] = un[k];
         }
@@ -382,12 +379,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) pr_pull_flat(PrArgs a) {
         for (int k = 0; k < UT; ++k) {
           const uint64_t i = r0 + lane + 32 * k;
           const bool ok = i < a.lr_arc1;
-          u[k] = ok ? ld_stream(a.col + i, stream) : 0u;
-          row[k] = ok ? row0 + ld_stream_u8(a.lr_rowd + (i - a.lr_arc0), stream) : 0xFFFFFFFFu;
+          u[k] = ok ? ldg(a.col + i) : 0u;
+          row[k] = ok ? row0 + (uint32_t)__ldg(a.lr_rowd + (i - a.lr_arc0)) : 0xFFFFFFFFu;
         }
         float x[UT];
 #pragma unroll
-        for (int k = 0; k < UT; ++k) x[k] = row[k] != 0xFFFFFFFFu ? ld_keep_f32(c_in + u[k], keep) : 0.f;
+        for (int k = 0; k < UT; ++k) x[k] = row[k] != 0xFFFFFFFFu ? c_in[u[k]] : 0.f;
 #pragma unroll
         for (int k = 0; k < UT; ++k) {
           if (seg_reduce(row[k] != 0xFFFFFFFFu, row[k], x[k])) atomicAdd(&acc_cur[row[k]], x[k]);
@@ -517,6 +514,106 @@ __global__ void __launch_bounds__(kBlock) pr_pull_residual_persistent(PrArgs a) 
     const uint32_t accum = *reinterpret_cast<volatile uint32_t*>(&ctl->active[it % 3]);
     if (gtid == 0) ctl->iters = it + 1;
     if (it + 1 >= a.max_iter || accum == 0) break;
+  }
+}
+
+// Pull-residual rounds for a degree-ordered graph: the flat light-row sweep
+// of pr_pull_flat gathering delta instead of the contribution.  A round's
+// vertex pass first folds the previous sweep's sums into the residual
+// (PageRank-pull.cpp:180-182: a positive sum replaces it), then takes the
+// residuals above tol into the value and writes the deltas (:163-172), so a
+// round is one vertex pass and one sweep with two grid barriers.  Rows with
+// no in-arcs (the no-in-arc tail) receive no sums: from round 2 on they are
+// skipped.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) pr_pull_residual_flat(PrArgs a) {
+  PrCtl* ctl = a.ctl;
+  const uint64_t deadline = kernel_deadline();
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const uint32_t lane = lane_id();
+  constexpr int UT = 8;
+  const uint64_t nruns = (a.lr_arc1 - a.lr_arc0 + 32 * UT - 1) / (32 * UT);
+  const uint64_t total = (uint64_t)a.sched.ntiles + nruns;
+  for (uint32_t it = 0;; ++it) {
+    float* const acc_prev = (it & 1) ? a.acc : a.acc2;  // the sums of round it-1
+    float* const acc_cur = (it & 1) ? a.acc2 : a.acc;
+    if (gtid == 0) ctl->active[(it + 1) % 3] = 0;
+    // vertex pass
+    uint32_t my_accum = 0;
+    // the tail's residuals are spent in round 0 and its deltas cleared in
+    // round 1 (they may have out-arcs: nout counts the stored columns)
+    const uint32_t vend = it >= 2 ? a.zero_from : a.n;
+    for (uint64_t v = gtid; v < vend; v += gthreads) {
+      float r = a.residual[v];
+      if (it > 0) {
+        const float sum = acc_prev[v];
+        acc_prev[v] = 0.f;
+        if (sum > 0.f) r = sum;
+      }
+      float d = 0.f;
+      if (r > a.tol) {
+        a.value[v] += r;
+        const uint32_t k = a.nout[v];
+        if (k > 0) {
+          d = r * a.alpha / (float)k;
+          ++my_accum;
+        }
+        r = 0.f;
+      }
+      a.residual[v] = r;
+      a.delta[v] = d;
+    }
+    my_accum = __reduce_add_sync(kFull, my_accum);
+    if (lane == 0 && my_accum) atomicAdd(&ctl->active[it % 3], my_accum);
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    const uint32_t accum = *reinterpret_cast<volatile uint32_t*>(&ctl->active[it % 3]);
+    if (gtid == 0) ctl->iters = it + 1;
+    // no delta anywhere: the sweep would add nothing (the round still counts)
+    if (accum == 0) break;
+    for (uint64_t t = gwarp; t < total; t += nwarps) {
+      if (t < a.sched.ntiles) {
+        const uint2 tv = a.sched.tiles[t];
+        const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
+        const uint64_t b = vb + (uint64_t)tv.y * a.sched.tile;
+        const uint64_t e = min(ve, b + a.sched.tile);
+        float sum = 0.f;
+        for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
+          uint32_t u[UT];
+#pragma unroll
+          for (int k = 0; k < UT; ++k) {
+            const uint64_t i = i0 + lane + 32 * k;
+            u[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
+          }
+#pragma unroll
+          for (int k = 0; k < UT; ++k) sum += u[k] != 0xFFFFFFFFu ? a.delta[u[k]] : 0.f;
+        }
+        sum = warp_sum(sum);
+        if (lane == 0 && sum > 0.f) atomicAdd(&acc_cur[tv.x], sum);
+      } else {
+        const uint64_t run = t - a.sched.ntiles;
+        const uint64_t r0 = a.lr_arc0 + run * kLightRun;
+        const uint32_t row0 = ldg(a.lr_runrow + run);
+        uint32_t u[UT], row[UT];
+#pragma unroll
+        for (int k = 0; k < UT; ++k) {
+          const uint64_t i = r0 + lane + 32 * k;
+          const bool ok = i < a.lr_arc1;
+          u[k] = ok ? ldg(a.col + i) : 0u;
+          row[k] = ok ? row0 + (uint32_t)__ldg(a.lr_rowd + (i - a.lr_arc0)) : 0xFFFFFFFFu;
+        }
+        float x[UT];
+#pragma unroll
+        for (int k = 0; k < UT; ++k) x[k] = row[k] != 0xFFFFFFFFu ? a.delta[u[k]] : 0.f;
+#pragma unroll
+        for (int k = 0; k < UT; ++k) {
+          if (seg_reduce(row[k] != 0xFFFFFFFFu, row[k], x[k]) && x[k] > 0.f) atomicAdd(&acc_cur[row[k]], x[k]);
+        }
+      }
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    if (it + 1 >= a.max_iter) break;  // the values are final; the last sums would only refill residuals
   }
 }
 
@@ -757,6 +854,42 @@ inline float bits_to_float(uint32_t u) {
   return f;
 }
 
+// The flat sweeps' run table of a degree-ordered graph (its heavy rows are
+// [0, nheavy), the light rows' arcs one contiguous range): built once per
+// heavy threshold and cached in the handle, then wired into `a`.
+int light_run_table(gb_graph* g, const SweepSched& sched, PrArgs* a, cudaStream_t s) {
+  if (!g->lr_rowid || g->lr_heavy != sched.heavy) {
+    cudaFree(g->lr_rowid);
+    g->lr_rowid = nullptr;
+    uint64_t ends[2] = {0, 0};
+    GB_CUDA(cudaMemcpyAsync(&ends[0], g->offs + sched.nheavy, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(&ends[1], g->offs + g->zero_from, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    if (ends[1] < ends[0]) GB_FAIL(GB_ERR_CUDA, "pagerank: light rows out of order");
+    // one allocation: the run rows (uint32 per run), then a byte per arc
+    const uint64_t narcs = ends[1] - ends[0];
+    const uint64_t nruns = (narcs + kLightRun - 1) / kLightRun;
+    GB_CUDA(cudaMalloc(&g->lr_rowid, sizeof(uint32_t) * std::max<uint64_t>(nruns, 1) + narcs + 16));
+    if (g->zero_from > sched.nheavy) {
+      uint32_t* runrow = g->lr_rowid;
+      uint8_t* rowd = reinterpret_cast<uint8_t*>(g->lr_rowid + std::max<uint64_t>(nruns, 1));
+      light_runrow_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, sched.nheavy, g->zero_from, ends[0], runrow);
+      light_rowd_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, sched.nheavy, g->zero_from, ends[0], runrow, rowd);
+    }
+    GB_CUDA(cudaGetLastError());
+    g->lr_row0 = sched.nheavy;
+    g->lr_heavy = sched.heavy;
+    g->lr_arc0 = ends[0];
+    g->lr_arc1 = ends[1];
+  }
+  a->lr_runrow = g->lr_rowid;
+  a->lr_rowd = reinterpret_cast<const uint8_t*>(
+      g->lr_rowid + std::max<uint64_t>((g->lr_arc1 - g->lr_arc0 + kLightRun - 1) / kLightRun, 1));
+  a->lr_arc0 = g->lr_arc0;
+  a->lr_arc1 = g->lr_arc1;
+  return GB_OK;
+}
+
 int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_iter, float* rank_out,
                  uint32_t* iters_out, gb_stats* stats, cudaStream_t s, float init = -1.f, float base = -1.f,
                  int linf = 0) {
@@ -826,43 +959,22 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
     kfn = reinterpret_cast<const void*>(&pr_pull_persistent<kBlock, 2, 6>);
     if (g->perm) {
       // degree-ordered: heavy rows are [0, nheavy), the light rows' arcs one
-      // contiguous range; their row ids are built once per heavy threshold
-      if (!g->lr_rowid || g->lr_heavy != sched.heavy) {
-        cudaFree(g->lr_rowid);
-        g->lr_rowid = nullptr;
-        uint64_t ends[2] = {0, 0};
-        GB_CUDA(cudaMemcpyAsync(&ends[0], g->offs + sched.nheavy, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        GB_CUDA(cudaMemcpyAsync(&ends[1], g->offs + g->zero_from, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        GB_CUDA(cudaStreamSynchronize(s));
-        if (ends[1] < ends[0]) GB_FAIL(GB_ERR_CUDA, "pagerank: light rows out of order");
-        // one allocation: the run rows (uint32 per run), then a byte per arc
-        const uint64_t narcs = ends[1] - ends[0];
-        const uint64_t nruns = (narcs + kLightRun - 1) / kLightRun;
-        GB_CUDA(cudaMalloc(&g->lr_rowid, sizeof(uint32_t) * std::max<uint64_t>(nruns, 1) + narcs + 16));
-        if (g->zero_from > sched.nheavy) {
-          uint32_t* runrow = g->lr_rowid;
-          uint8_t* rowd = reinterpret_cast<uint8_t*>(g->lr_rowid + std::max<uint64_t>(nruns, 1));
-          light_runrow_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, sched.nheavy, g->zero_from, ends[0], runrow);
-          light_rowd_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, sched.nheavy, g->zero_from, ends[0], runrow,
-                                                              rowd);
-        }
-        GB_CUDA(cudaGetLastError());
-        g->lr_row0 = sched.nheavy;
-        g->lr_heavy = sched.heavy;
-        g->lr_arc0 = ends[0];
-        g->lr_arc1 = ends[1];
-      }
-      a.lr_runrow = g->lr_rowid;
-      a.lr_rowd = reinterpret_cast<const uint8_t*>(
-          g->lr_rowid + std::max<uint64_t>((g->lr_arc1 - g->lr_arc0 + kLightRun - 1) / kLightRun, 1));
-      a.lr_arc0 = g->lr_arc0;
-      a.lr_arc1 = g->lr_arc1;
+      // contiguous range swept flat
+      st = light_run_table(g, sched, &a, s);
+      if (st != GB_OK) return st;
       kfn = reinterpret_cast<const void*>(&pr_pull_flat<kBlock, 6>);
     }
   } else if (kind == PrKind::PullResidual) {
     pr_resid_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     GB_CUDA(cudaMemsetAsync(a.acc, 0, sizeof(float) * n, s));
+    GB_CUDA(cudaMemsetAsync(a.acc2, 0, sizeof(float) * n, s));
     kfn = reinterpret_cast<const void*>(&pr_pull_residual_persistent);
+    if (g->perm) {
+      a.zero_from = g->zero_from;
+      st = light_run_table(g, sched, &a, s);
+      if (st != GB_OK) return st;
+      kfn = reinterpret_cast<const void*>(&pr_pull_residual_flat<kBlock, 6>);
+    }
   } else if (kind == PrKind::Push) {
     pr_push_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     kfn = reinterpret_cast<const void*>(&pr_push_persistent);

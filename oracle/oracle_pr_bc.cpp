@@ -76,8 +76,12 @@ uint32_t pr_pull_residual(const Csr& g, uint64_t m, T alpha, T tol, uint32_t max
   for (uint32_t v = 0; v < n; ++v) value[v] = 0;
   uint32_t iterations = 0;
   while (true) {
-    uint32_t accum = 0;
-    for (uint32_t v = 0; v < n; ++v) {
+    // both loops are per-vertex and read only what the other loop wrote, so
+    // the parallel form gives the serial result
+    uint64_t accum = 0;
+#pragma omp parallel for schedule(static) reduction(+ : accum)
+    for (int64_t vv = 0; vv < (int64_t)n; ++vv) {
+      const uint32_t v = (uint32_t)vv;
       delta[v] = 0;
       if (residual[v] > tol) {
         const T old = residual[v];
@@ -89,7 +93,9 @@ uint32_t pr_pull_residual(const Csr& g, uint64_t m, T alpha, T tol, uint32_t max
         }
       }
     }
-    for (uint32_t v = 0; v < n; ++v) {
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t vv = 0; vv < (int64_t)n; ++vv) {
+      const uint32_t v = (uint32_t)vv;
       T sum = 0;
       for (uint64_t i = g.b(v); i < g.e(v); ++i) {
         const T d = delta[g.col[i]];

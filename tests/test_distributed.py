@@ -173,3 +173,92 @@ def test_clock_sampler_merges_fast_samples():
     assert got["sm_max_mhz"] == 1965.0
     assert got["reasons"] == ["sw_power_cap"]
     assert got["samples_nvml"] >= 3
+
+
+def test_shard_columns_blocks_of_four():
+    from galois_b200.distributed import shard_columns
+
+    for B in (4, 8, 128, 12):
+        for world in (1, 2, 3, 4, 8):
+            parts = [shard_columns(B, r, world) for r in range(world)]
+            cols = [c for a, b in parts for c in range(a, b)]
+            assert cols == list(range(B))  # contiguous, no gap, no overlap
+            assert all((b - a) % 4 == 0 for a, b in parts)
+    assert shard_columns(1, 0, 2) == (0, 1) and shard_columns(1, 1, 2) == (0, 0)
+    assert shard_columns(128, 1, 2) == (64, 128)
+    with pytest.raises(ValueError):
+        shard_columns(6, 0, 2)
+
+
+def _dense_ppr(graph, T, w, alpha, tol, max_iter):
+    """Stand-in for the GPU solve on the host: the same system
+    x = (1-alpha) T + alpha W~ x with W~_ij = w_ji / s_j, solved densely in
+    FP64 by torch (differentiable in T and w)."""
+    import torch
+
+    src, dst = graph
+    n = T.shape[0]
+    s = torch.zeros(n, dtype=w.dtype).index_add(0, src, w)
+    vals = w / s[src]
+    W = torch.zeros((n, n), dtype=w.dtype).index_put((dst, src), vals, accumulate=True)
+    A = torch.eye(n, dtype=w.dtype) - alpha * W
+    return torch.linalg.solve(A, (1 - alpha) * T)
+
+
+def _ppr_rank(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from galois_b200.distributed import ppr_sharded
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        g = torch.Generator().manual_seed(3)
+        n, m, B = 30, 120, 12
+        src = torch.randint(0, n, (m,), generator=g)
+        dst = torch.randint(0, n, (m,), generator=g)
+        w = torch.rand(m, generator=g, dtype=torch.float64) + 0.1
+        T = torch.rand((n, B), generator=g, dtype=torch.float64)
+        c = torch.randn((n, B), generator=g, dtype=torch.float64)
+        x, cols, gt, gw, loss = ppr_sharded((src, dst), T, w, c, solve=_dense_ppr)
+        q.put((rank, cols, x.tolist(), gt.tolist(), gw.tolist(), float(loss)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_ppr_columns_sharded_and_grad_w_reduced():
+    """Two gloo ranks each solve half of the teleport columns; the all-reduced
+    edge-weight gradient and the summed loss equal one process solving all
+    columns, and the per-rank columns equal the matching columns of the
+    whole solve."""
+    import torch
+
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_ppr_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    g = torch.Generator().manual_seed(3)
+    n, m, B = 30, 120, 12
+    src = torch.randint(0, n, (m,), generator=g)
+    dst = torch.randint(0, n, (m,), generator=g)
+    w = (torch.rand(m, generator=g, dtype=torch.float64) + 0.1).requires_grad_(True)
+    T = torch.rand((n, B), generator=g, dtype=torch.float64).requires_grad_(True)
+    c = torch.randn((n, B), generator=g, dtype=torch.float64)
+    x = _dense_ppr((src, dst), T, w, 0.85, 0, 0)
+    loss = (c * x).sum()
+    loss.backward()
+    assert [r[1] for r in res] == [(0, 4), (4, 12)] or [r[1] for r in res] == [(0, 8), (8, 12)]
+    for rank, (b0, b1), xl, gtl, gw, tot in res:
+        assert torch.allclose(torch.tensor(xl, dtype=torch.float64), x.detach()[:, b0:b1])
+        assert torch.allclose(torch.tensor(gtl, dtype=torch.float64), T.grad[:, b0:b1])
+        assert torch.allclose(torch.tensor(gw, dtype=torch.float64), w.grad)
+        assert abs(tot - float(loss)) < 1e-9 * max(1.0, abs(float(loss)))

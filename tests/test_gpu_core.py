@@ -300,9 +300,10 @@ RESIDUAL = [("pull-residual", "pagerank_pull_residual", oracle.pr_pull_residual)
             ("push-sync", "pagerank_push", oracle.pr_push_sync)]
 
 
+@pytest.mark.parametrize("reorder", [0, 1])
 @pytest.mark.parametrize("name,method,restated", RESIDUAL)
 @pytest.mark.parametrize("scale,ef,seed,tol", [(12, 8, 19, 1e-3), (12, 8, 17, 1e-4), (14, 16, 41, 1e-4)])
-def test_pagerank_residual_vs_restatement(cuda_device, name, method, restated, scale, ef, seed, tol):
+def test_pagerank_residual_vs_restatement(cuda_device, name, method, restated, scale, ef, seed, tol, reorder):
     """The residual variants against the oracle's FP64 restatement of the same
     rounds (PageRank-pull.cpp:132-190, PageRank-push.cpp:103-188) at the same
     tolerance: <= 1e-5 relative per vertex (absolute below 1), and the same
@@ -311,7 +312,8 @@ def test_pagerank_residual_vs_restatement(cuda_device, name, method, restated, s
     apart; the bound holds with that slack (measured <= 3e-6)."""
     g, _ = rmat(scale, ef, seed=seed)
     want, it64 = restated(g, 0.85, tol, 1000, f64=True)
-    with DeviceGraph(g, symmetric=True) as dg:
+    # reorder 1: the degree-ordered graph (the flat light-row sweep for pull-residual)
+    with DeviceGraph(g, symmetric=True, reorder=reorder) as dg:
         got, st = getattr(dg, method)(0.85, tol, 1000, stats=True)
     assert _rel(got, want) <= 1e-5, name
     assert abs(st["iterations"] - it64) <= 2, f"{name}: {st['iterations']} rounds vs {it64}"

@@ -114,3 +114,44 @@ def test_autograd_matches_fp64_and_finite_differences(cuda_device):
                 lm = float((ct * ppr(dg, Tt.detach(), wm, ALPHA, 1e-7)).sum())
             fd = (lp - lm) / (2 * h)
             assert abs(fd - gw_ref[e]) <= 5e-2 * abs(gw_ref[e]) + 1e-4
+
+
+def test_ppr_sharded_single_rank_matches_autograd(cuda_device):
+    """galois_b200.distributed.ppr_sharded over a one-rank NCCL group gives
+    the plain autograd result (the multi-rank split and the all-reduce of
+    grad_w are covered by the gloo tests)."""
+    import datetime
+    import os
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from galois_b200.distributed import ppr_sharded
+    from galois_b200.ppr import ppr
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    try:
+        g, T, c = setup(scale=10, B=8)
+        with DeviceGraph(g) as dg:
+            Tt = torch.from_numpy(T).cuda()
+            ct = torch.from_numpy(c).cuda()
+            w = torch.from_numpy(g.w_f32).cuda()
+            x, cols, gt, gw, loss = ppr_sharded(dg, Tt, w, ct, ALPHA, 1e-7)
+            wr = w.clone().requires_grad_(True)
+            Tr = Tt.clone().requires_grad_(True)
+            xr = ppr(dg, Tr, wr, ALPHA, 1e-7)
+            lr = (ct * xr).sum()
+            lr.backward()
+        assert cols == (0, 8)
+        assert torch.allclose(x, xr.detach())
+        assert torch.allclose(gt, Tr.grad)
+        assert torch.allclose(gw, wr.grad)
+        assert abs(float(loss) - float(lr)) <= 1e-5 * max(1.0, abs(float(lr)))
+    finally:
+        dist.destroy_process_group()
