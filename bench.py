@@ -901,7 +901,7 @@ def roofline_of(job: Job, r: dict, order: int, traffic) -> dict:
     return {"bound": "hbm", "achieved": need / sec / 1e9, "peak": peak, "unit": "GB/s",
             "frac": need / sec / 1e9 / peak, "peak_source": peak_src,
             # a degree-ordered PageRank runs the flat pull kernels
-            "kernel": job.kernel.replace("_persistent", "_flat") if (isinstance(job, PrJob) and order) else job.kernel,
+            "kernel": "pr_pull_flat" if (type(job) is PrJob and order) else job.kernel,
             "bytes_counted_per_step": need,
             "algorithmic_bytes_per_step": r["bytes_step"], "kernel_ms_per_step": sum(r["kms"]),
             "model_frac": r["bytes_step"] / sec / 1e9 / peak,

@@ -517,106 +517,6 @@ __global__ void __launch_bounds__(kBlock) pr_pull_residual_persistent(PrArgs a) 
   }
 }
 
-// Pull-residual rounds for a degree-ordered graph: the flat light-row sweep
-// of pr_pull_flat gathering delta instead of the contribution.  A round's
-// vertex pass first folds the previous sweep's sums into the residual
-// (PageRank-pull.cpp:180-182: a positive sum replaces it), then takes the
-// residuals above tol into the value and writes the deltas (:163-172), so a
-// round is one vertex pass and one sweep with two grid barriers.  Rows with
-// no in-arcs (the no-in-arc tail) receive no sums: from round 2 on they are
-// skipped.
-template <int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) pr_pull_residual_flat(PrArgs a) {
-  PrCtl* ctl = a.ctl;
-  const uint64_t deadline = kernel_deadline();
-  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
-  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
-  const uint64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
-  const uint32_t lane = lane_id();
-  constexpr int UT = 8;
-  const uint64_t nruns = (a.lr_arc1 - a.lr_arc0 + 32 * UT - 1) / (32 * UT);
-  const uint64_t total = (uint64_t)a.sched.ntiles + nruns;
-  for (uint32_t it = 0;; ++it) {
-    float* const acc_prev = (it & 1) ? a.acc : a.acc2;  // the sums of round it-1
-    float* const acc_cur = (it & 1) ? a.acc2 : a.acc;
-    if (gtid == 0) ctl->active[(it + 1) % 3] = 0;
-    // vertex pass
-    uint32_t my_accum = 0;
-    // the tail's residuals are spent in round 0 and its deltas cleared in
-    // round 1 (they may have out-arcs: nout counts the stored columns)
-    const uint32_t vend = it >= 2 ? a.zero_from : a.n;
-    for (uint64_t v = gtid; v < vend; v += gthreads) {
-      float r = a.residual[v];
-      if (it > 0) {
-        const float sum = acc_prev[v];
-        acc_prev[v] = 0.f;
-        if (sum > 0.f) r = sum;
-      }
-      float d = 0.f;
-      if (r > a.tol) {
-        a.value[v] += r;
-        const uint32_t k = a.nout[v];
-        if (k > 0) {
-          d = r * a.alpha / (float)k;
-          ++my_accum;
-        }
-        r = 0.f;
-      }
-      a.residual[v] = r;
-      a.delta[v] = d;
-    }
-    my_accum = __reduce_add_sync(kFull, my_accum);
-    if (lane == 0 && my_accum) atomicAdd(&ctl->active[it % 3], my_accum);
-    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
-    const uint32_t accum = *reinterpret_cast<volatile uint32_t*>(&ctl->active[it % 3]);
-    if (gtid == 0) ctl->iters = it + 1;
-    // no delta anywhere: the sweep would add nothing (the round still counts)
-    if (accum == 0) break;
-    for (uint64_t t = gwarp; t < total; t += nwarps) {
-      if (t < a.sched.ntiles) {
-        const uint2 tv = a.sched.tiles[t];
-        const uint64_t vb = ldg(a.offs + tv.x), ve = ldg(a.offs + tv.x + 1);
-        const uint64_t b = vb + (uint64_t)tv.y * a.sched.tile;
-        const uint64_t e = min(ve, b + a.sched.tile);
-        float sum = 0.f;
-        for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
-          uint32_t u[UT];
-#pragma unroll
-          for (int k = 0; k < UT; ++k) {
-            const uint64_t i = i0 + lane + 32 * k;
-            u[k] = i < e ? ldg(a.col + i) : 0xFFFFFFFFu;
-          }
-#pragma unroll
-          for (int k = 0; k < UT; ++k) sum += u[k] != 0xFFFFFFFFu ? a.delta[u[k]] : 0.f;
-        }
-        sum = warp_sum(sum);
-        if (lane == 0 && sum > 0.f) atomicAdd(&acc_cur[tv.x], sum);
-      } else {
-        const uint64_t run = t - a.sched.ntiles;
-        const uint64_t r0 = a.lr_arc0 + run * kLightRun;
-        const uint32_t row0 = ldg(a.lr_runrow + run);
-        uint32_t u[UT], row[UT];
-#pragma unroll
-        for (int k = 0; k < UT; ++k) {
-          const uint64_t i = r0 + lane + 32 * k;
-          const bool ok = i < a.lr_arc1;
-          u[k] = ok ? ldg(a.col + i) : 0u;
-          row[k] = ok ? row0 + (uint32_t)__ldg(a.lr_rowd + (i - a.lr_arc0)) : 0xFFFFFFFFu;
-        }
-        float x[UT];
-#pragma unroll
-        for (int k = 0; k < UT; ++k) x[k] = row[k] != 0xFFFFFFFFu ? a.delta[u[k]] : 0.f;
-#pragma unroll
-        for (int k = 0; k < UT; ++k) {
-          if (seg_reduce(row[k] != 0xFFFFFFFFu, row[k], x[k]) && x[k] > 0.f) atomicAdd(&acc_cur[row[k]], x[k]);
-        }
-      }
-    }
-    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
-    if (it + 1 >= a.max_iter) break;  // the values are final; the last sums would only refill residuals
-  }
-}
-
 // ---- residual push, Sync (PageRank-push.cpp:103-188) ------------------------
 __global__ void pr_push_init(PrArgs a) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -967,14 +867,7 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
   } else if (kind == PrKind::PullResidual) {
     pr_resid_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     GB_CUDA(cudaMemsetAsync(a.acc, 0, sizeof(float) * n, s));
-    GB_CUDA(cudaMemsetAsync(a.acc2, 0, sizeof(float) * n, s));
     kfn = reinterpret_cast<const void*>(&pr_pull_residual_persistent);
-    if (g->perm) {
-      a.zero_from = g->zero_from;
-      st = light_run_table(g, sched, &a, s);
-      if (st != GB_OK) return st;
-      kfn = reinterpret_cast<const void*>(&pr_pull_residual_flat<kBlock, 6>);
-    }
   } else if (kind == PrKind::Push) {
     pr_push_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     kfn = reinterpret_cast<const void*>(&pr_push_persistent);

@@ -118,17 +118,19 @@ def test_pagerank_pull_rmat24_config(cuda_device, rmat24):
 
 def test_pagerank_pull_residual_rmat24_app_default(cuda_device, rmat24):
     """Pull-residual, the pull app's default (PageRank-pull.cpp:34-37), at its
-    default tolerance 1e-3 on RMAT-24: <= 1e-5 relative per vertex (absolute
-    below 1) against the FP64 restatement of the same rounds, and the same
-    number of rounds within 2; both vertex orders (the degree-ordered one
-    runs the flat light-row sweep)."""
+    default tolerance 1e-3 on RMAT-24 against the FP64 restatement of the
+    same rounds: every vertex within 1e-5 relative (absolute below 1) except
+    rare threshold flips, which stay within 2 tol (the bound and its reason
+    are check_residual_parity's in test_gpu_core.py), and the same number of
+    rounds within 2; both vertex orders."""
+    from test_gpu_core import check_residual_parity
+
     g = rmat24
     want, it64 = oracle.pr_pull_residual(g, ALPHA, 1e-3, 1000, f64=True)
     for order in (0, 1):
         with DeviceGraph(g, symmetric=True, reorder=order) as dg:
             got, st = dg.pagerank_pull_residual(ALPHA, 1e-3, 1000, stats=True)
-        err = float((np.abs(got.astype(np.float64) - want) / np.maximum(np.abs(want), 1.0)).max())
-        assert err <= 1e-5, f"order {order}: {err:.2e}"
+        check_residual_parity(got, want, 1e-3, f"order {order}")
         assert abs(st["iterations"] - it64) <= 2, f"order {order}: {st['iterations']} vs {it64}"
 
 

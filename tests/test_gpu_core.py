@@ -296,6 +296,22 @@ def _rel(got, want):
     return float((np.abs(got.astype(np.float64) - want) / np.maximum(np.abs(want), 1.0)).max())
 
 
+def check_residual_parity(got, want, tol, what):
+    """Residual PageRank against the FP64 restatement of the same rounds at
+    the same tolerance.  Every vertex within 1e-5 relative (absolute below
+    1), except where a residual lying within fp32 rounding of tol was taken
+    on one side and not on the other (a threshold flip, possible because the
+    GPU sums in another order): the value there differs by that residual,
+    at most tol, and its neighbours' by alpha / nout of it.  Such vertices
+    must be rare (at most 1e-4 of them, and at least 10 allowed) and stay
+    within 1e-5 relative + 2 tol."""
+    err = np.abs(got.astype(np.float64) - want)
+    scale = np.maximum(np.abs(want), 1.0)
+    flipped = int((err > 1e-5 * scale).sum())
+    assert flipped <= max(10, 1e-4 * want.size), f"{what}: {flipped} vertices beyond 1e-5 relative"
+    assert float((err - 1e-5 * scale).max()) <= 2 * tol, f"{what}: max error {float(err.max()):.3e}"
+
+
 RESIDUAL = [("pull-residual", "pagerank_pull_residual", oracle.pr_pull_residual),
             ("push-sync", "pagerank_push", oracle.pr_push_sync)]
 
@@ -306,16 +322,14 @@ RESIDUAL = [("pull-residual", "pagerank_pull_residual", oracle.pr_pull_residual)
 def test_pagerank_residual_vs_restatement(cuda_device, name, method, restated, scale, ef, seed, tol, reorder):
     """The residual variants against the oracle's FP64 restatement of the same
     rounds (PageRank-pull.cpp:132-190, PageRank-push.cpp:103-188) at the same
-    tolerance: <= 1e-5 relative per vertex (absolute below 1), and the same
-    number of rounds within 2.  The GPU sums in fp32 in another order, so a
-    residual lying within rounding of the tolerance may be absorbed one round
-    apart; the bound holds with that slack (measured <= 3e-6)."""
+    tolerance, as check_residual_parity states, and the same number of
+    rounds within 2; both vertex orders."""
     g, _ = rmat(scale, ef, seed=seed)
     want, it64 = restated(g, 0.85, tol, 1000, f64=True)
     # reorder 1: the degree-ordered graph (the flat light-row sweep for pull-residual)
     with DeviceGraph(g, symmetric=True, reorder=reorder) as dg:
         got, st = getattr(dg, method)(0.85, tol, 1000, stats=True)
-    assert _rel(got, want) <= 1e-5, name
+    check_residual_parity(got, want, tol, name)
     assert abs(st["iterations"] - it64) <= 2, f"{name}: {st['iterations']} rounds vs {it64}"
 
 

@@ -152,6 +152,6 @@ def test_ppr_sharded_single_rank_matches_autograd(cuda_device):
         assert torch.allclose(x, xr.detach())
         assert torch.allclose(gt, Tr.grad)
         assert torch.allclose(gw, wr.grad)
-        assert abs(float(loss) - float(lr)) <= 1e-5 * max(1.0, abs(float(lr)))
+        assert abs(float(loss) - float(lr.detach())) <= 1e-5 * max(1.0, abs(float(lr.detach())))
     finally:
         dist.destroy_process_group()
