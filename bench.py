@@ -921,12 +921,13 @@ def run_apps(args, dev: int) -> dict:
 
     single = Dist(want_pg=False)
     g24, _ = rmat(24, 16, seed=24, symmetrize=True)
-    jobs = [("bfs-rmat20", BfsJob("full")),
-            ("bfs-rmat24", BfsJob("full", graph=g24, name="rmat24-sym")),
-            ("cc-rmat24", CcJob("full", graph=g24, name="rmat24-sym")),
-            ("pr-rmat24", PrJob("full", graph=g24, name="rmat24-sym"))]
+    # (key, job, its DRAM traffic entry in profiles/traffic.json)
+    jobs = [("bfs-rmat20", BfsJob("full"), "bfs-full"),
+            ("bfs-rmat24", BfsJob("full", graph=g24, name="rmat24-sym"), "bfs-s24"),
+            ("cc-rmat24", CcJob("full", graph=g24, name="rmat24-sym"), "cc-full"),
+            ("pr-rmat24", PrJob("full", graph=g24, name="rmat24-sym"), "pr-full")]
     out = {}
-    for key, job in jobs:
+    for key, job, traffic_key in jobs:
         r = measure_resident(job, dev, single, args.steps, args.warmup, args.order)
         gpu_host = r["outs"][0].cpu().numpy()
         for dg in r["dgs"]:
@@ -945,7 +946,8 @@ def run_apps(args, dev: int) -> dict:
                     "m": job.graphs[0]["host"].m, "metric": job.metric,
                     "value": r["units_step"] * args.steps / (r["t_ms"] / 1e3) / 1e9, "unit": job.unit,
                     "ms_per_step": r["t_ms"] / args.steps, "kernel_ms": sum(r["kms"]),
-                    "roofline": roofline_of(job, r, args.order, None), "clocks": r["clocks"],
+                    "roofline": roofline_of(job, r, args.order, traffic_from_profiles(traffic_key)),
+                    "clocks": r["clocks"],
                     "parity": job.check(gpu_host, 0),
                     "stats": {k: st[k] for k in ("vertices_reached", "edges_reached", "edges_scanned", "rounds",
                                                  "pull_rounds", "iterations") if k in st},
