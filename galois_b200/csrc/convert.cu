@@ -261,6 +261,9 @@ int gb_graph_assign_weights_u32(gb_graph* g, uint32_t lo, uint32_t hi, uint64_t 
     cudaError_t e = pool_malloc(reinterpret_cast<void**>(&g->w), sizeof(uint32_t) * std::max<uint64_t>(g->m, 1));
     if (e != cudaSuccess) return cuda_fail(e, "gb_graph_assign_weights_u32");
   }
+  cudaFree(g->ell);  // its rows carry the weights
+  g->ell = nullptr;
+  g->ell_d = 0;
   if (g->m)
     weights_u32_kernel<<<grid_for(g, g->m), 256, 0, s>>>(g->w, g->m, stream_key(seed, kTagWeightU32), lo,
                                                          (uint64_t)hi - lo + 1);
@@ -297,6 +300,9 @@ int gb_graph_assign_weights_reference(gb_graph* g, int min_value, int max_value,
   GB_CUDA(cudaSetDevice(g->device));
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (edge_bytes == -4) drop_derived(g);  // float weights feed the transpose's copy and the PPR state
+  cudaFree(g->ell);                       // uint32 weights ride in the fixed-width rows
+  g->ell = nullptr;
+  g->ell_d = 0;
   void** dst = edge_bytes == 4 ? reinterpret_cast<void**>(&g->w) : reinterpret_cast<void**>(&g->wf);
   const size_t bytes = 4 * std::max<uint64_t>(g->m, 1);
   if (!*dst) {

@@ -42,6 +42,10 @@ struct gb_graph {
   uint32_t lr_row0 = 0, lr_heavy = 0;
   uint64_t lr_arc0 = 0, lr_arc1 = 0;
   float* colsum = nullptr;               // PPR column sums of wf by source
+  // bounded-degree graphs: the arcs as fixed-width rows (ell_d slots per
+  // vertex, columns then uint32 weights, empty slots 0xFFFFFFFF), for SSSP
+  uint32_t* ell = nullptr;
+  uint32_t ell_d = 0;
   uint32_t max_degree = 0;
   // all-vertex sweep schedule (sweep.cuh), cached per (heavy, tile)
   uint2* sweep_tiles = nullptr;

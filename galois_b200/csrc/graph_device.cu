@@ -405,6 +405,7 @@ int gb_graph_free(gb_graph* g) {
   cudaFree(g->outdeg_of_stored);
   cudaFree(g->lr_rowid);
   cudaFree(g->colsum);
+  cudaFree(g->ell);
   if (g->ppr_free) g->ppr_free(g);
   cudaFree(g->sweep_tiles);
   cudaFree(g->sweep_heavy_list);

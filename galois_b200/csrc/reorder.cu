@@ -144,6 +144,9 @@ void drop_derived(gb_graph* g) {
   cudaFree(g->colsum);
   g->outdeg_of_stored = nullptr;
   g->colsum = nullptr;
+  cudaFree(g->ell);
+  g->ell = nullptr;
+  g->ell_d = 0;
   cudaFree(g->sweep_tiles);
   cudaFree(g->sweep_heavy_list);
   g->sweep_tiles = nullptr;

@@ -674,6 +674,241 @@ __global__ void __launch_bounds__(BLOCK) sssp_async(SsspArgs a) {
   if (gtid == 0) ctl->phases = P;
 }
 
+// ---- asynchronous buckets over fixed-width rows ------------------------------
+// For graphs of degree <= D (D = 4 or 8) the arcs are also kept as
+// fixed-width rows: vertex u's D columns at ell[u*D ..], its D weights at
+// ell[n*D + u*D ..], empty slots 0xFFFFFFFF.  A row's address follows from
+// the vertex id alone, so a relaxation loads the target's row beside its
+// atomicMin, and a queued entry carries the row it will expand: one hop of
+// the dependent chain is one memory round trip (the atomic and the row load
+// in flight together) instead of two (arcs, then atomics).  D lanes work on
+// one vertex (lane k on its k-th slot), 32 / D vertices per round.
+
+constexpr uint32_t kNoArc = 0xFFFFFFFFu;
+
+__global__ void ell_build_kernel(const uint64_t* __restrict__ offs, const uint32_t* __restrict__ col,
+                                 const uint32_t* __restrict__ w, uint32_t n, uint32_t D, uint32_t* __restrict__ ell) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < (uint64_t)n * D; i += stride) {
+    const uint64_t v = i / D, k = i % D;
+    const uint64_t b = offs[v], deg = offs[v + 1] - b;
+    ell[i] = k < deg ? col[b + k] : kNoArc;
+    ell[(uint64_t)n * D + i] = k < deg ? w[b + k] : kNoArc;
+  }
+}
+
+template <int D>
+struct EllRow {
+  uint4 c[D / 4];
+  uint4 w[D / 4];
+};
+
+template <int D>
+__device__ __forceinline__ EllRow<D> ell_row(const uint32_t* __restrict__ ell, uint32_t n, uint32_t u) {
+  EllRow<D> r;
+  const uint4* pc = reinterpret_cast<const uint4*>(ell + (uint64_t)u * D);
+  const uint4* pw = reinterpret_cast<const uint4*>(ell + (uint64_t)n * D + (uint64_t)u * D);
+#pragma unroll
+  for (int j = 0; j < D / 4; ++j) {
+    r.c[j] = ldg(pc + j);
+    r.w[j] = ldg(pw + j);
+  }
+  return r;
+}
+
+__device__ __forceinline__ uint32_t u4_at(const uint4& v, uint32_t k) {
+  return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+}
+
+constexpr int kEllLQ = 64;  // local-queue entries per warp
+
+template <int BLOCK, int D>
+__global__ void __launch_bounds__(BLOCK) sssp_async_ell(SsspArgs a, const uint32_t* __restrict__ ell) {
+  static_assert(D == 4 || D == 8, "rows of 4 or 8 slots");
+  constexpr uint32_t kPer = 32 / D;  // vertices per round
+  __shared__ uint2 s_meta[BLOCK / 32][kEllLQ];  // (vertex, distance)
+  __shared__ EllRow<D> s_row[BLOCK / 32][kEllLQ];
+  SsspCtl* ctl = a.ctl;
+  worklists::RingCtl* rc = a.ring.rc;
+  const unsigned nblocks = gridDim.x;
+  const uint64_t deadline = kernel_deadline();
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  const uint32_t slot = lane / D, k = lane % D;
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  uint2* meta = s_meta[wib];
+  EllRow<D>* rows = s_row[wib];
+  unsigned long long my_scanned = 0, my_relax = 0;
+  uint32_t bucket = 0;
+  int fp = 0;
+  uint32_t P = 0;
+  for (;;) {
+    if (P >= a.max_phases) {
+      if (gtid == 0) raise_err(&ctl->err, kDevMaxRounds);
+      break;
+    }
+    const uint64_t hi64 = ((uint64_t)bucket + 1) << a.shift;
+    const uint32_t hi = hi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)hi64;
+    uint32_t* farq = a.far[fp];
+    uint32_t lq_n = 0;  // warp-uniform
+    bool busy = false;  // this warp holds one count of rc->work
+    // the 32 oldest local entries leave as one ring chunk of (vertex, distance)
+    auto spill_oldest = [&]() {
+      const uint2 e = meta[lane];
+      __syncwarp();
+      for (uint32_t i = 32 + lane; i < lq_n; i += 32) {
+        meta[i - 32] = meta[i];
+        rows[i - 32] = rows[i];
+      }
+      __syncwarp();
+      lq_n -= 32;
+      worklists::publish(a.ring, true, make_uint4(e.x, e.y, 0u, 0u), &ctl->err);
+    };
+    for (;;) {
+      uint32_t v = 0, dv = 0, u = 0, w = 0;
+      bool has = false;
+      if (lq_n == 0) {
+        // out of work: give up this warp's count, take a ticket, wait for a chunk
+        if (busy && lane == 0) atomicSub(&rc->work, 1);
+        busy = false;
+        unsigned long long p = 0;
+        int got = 0;
+        if (lane == 0) {
+          p = atomicAdd(&rc->head, 1ull);
+          got = worklists::wait_chunk(a.ring, p, &ctl->err, deadline);
+        }
+        got = __shfl_sync(kFull, got, 0);
+        if (got <= 0) break;  // the bucket is done (or an error was raised)
+        p = __shfl_sync(kFull, p, 0);
+        __syncwarp();
+        busy = true;
+        const unsigned long long cs = p & a.ring.mask;
+        const uint32_t c = __ldcg(a.ring.cnt + cs);
+        if (lane < c) {
+          const uint4 e = __ldcg(a.ring.ent + cs * 32 + lane);
+          meta[lane] = make_uint2(e.x, e.y);
+          rows[lane] = ell_row<D>(ell, a.n, e.x);
+        }
+        __syncwarp();
+        if (lane == 0) worklists::st_release(a.ring.seq + cs, p + a.ring.mask + 1);
+        lq_n = c;
+      }
+      // one round: the kPer most recent entries, lane k on slot k of its vertex
+      const uint32_t take = min(kPer, lq_n);
+      has = slot < take;
+      if (has) {
+        const uint32_t idx = lq_n - take + slot;
+        const uint2 m = meta[idx];
+        v = m.x;
+        dv = m.y;
+        u = u4_at(rows[idx].c[k >> 2], k & 3);
+        w = u4_at(rows[idx].w[k >> 2], k & 3);
+      }
+      __syncwarp();
+      lq_n -= take;
+      const bool valid = has && u != kNoArc;
+      const uint32_t nd = dv + w;
+      // in flight together: the entry's own distance (stale check), the
+      // target's atomic and the target's row
+      const uint32_t cur = (has && k == 0) ? __ldcg(a.dist + v) : 0u;
+      uint32_t old = 0;
+      EllRow<D> nr{};
+      if (valid) {
+        old = atomicMin(&a.dist[u], nd);
+        nr = ell_row<D>(ell, a.n, u);
+      }
+      const bool live = __shfl_sync(kFull, cur, lane & ~(D - 1)) >= dv;
+      const bool improved = valid && live && nd < old;
+      if (valid && live) ++my_scanned;
+      bool near = false, far = false;
+      if (improved) {
+        ++my_relax;
+        if (nd < hi) {
+          near = nr.c[0].x != kNoArc;  // nothing to relax from a vertex without arcs
+        } else {
+          const uint32_t bit = 1u << (u & 31);
+          if (!(a.infar[u >> 5] & bit)) far = !(atomicOr(&a.infar[u >> 5], bit) & bit);
+        }
+      }
+      const unsigned nm = __ballot_sync(kFull, near);
+      if (nm) {
+        const uint32_t kk = __popc(nm);
+        if (lq_n + kk > (uint32_t)kEllLQ) spill_oldest();
+        if (near) {
+          const uint32_t pos = lq_n + __popc(nm & lanemask_lt);
+          meta[pos] = make_uint2(u, nd);
+          rows[pos] = nr;
+        }
+        lq_n += kk;
+        __syncwarp();
+      }
+      warp_push(far, u, farq, &ctl->far_count[fp], a.n, &ctl->err);
+      // while other warps wait for work, hand them the oldest entries
+      if (lq_n > 32) {
+        int want = 0;
+        if (lane == 0)
+          want = *reinterpret_cast<const volatile unsigned long long*>(&rc->head) >
+                 *reinterpret_cast<const volatile unsigned long long*>(&rc->tail);
+        if (__shfl_sync(kFull, want, 0)) spill_oldest();
+      }
+    }
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    // ---- bucket transition (as sssp_async) --------------------------------------
+    const uint32_t nfar = min(ctl->far_count[fp], a.n);
+    ++P;
+    if (nfar == 0) break;
+    if (gtid == 0) {
+      rc->head = rc->tail;
+      ctl->min_bucket = 0xFFFFFFFFu;
+      ctl->buckets += 1;
+      ctl->far_count[fp ^ 1] = 0;
+    }
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    {
+      uint32_t mb = 0xFFFFFFFFu;
+      for (uint64_t i = gtid; i < nfar; i += gthreads) {
+        const uint32_t dd = a.dist[farq[i]];
+        if (dd >= hi) mb = min(mb, dd >> a.shift);
+      }
+      mb = __reduce_min_sync(kFull, mb);
+      if (lane == 0 && mb != 0xFFFFFFFFu) atomicMin(&ctl->min_bucket, mb);
+    }
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+    const uint32_t nb = ctl->min_bucket;
+    if (nb == 0xFFFFFFFFu) break;
+    {
+      const uint64_t nhi64 = ((uint64_t)nb + 1) << a.shift;
+      const uint32_t nhi = nhi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)nhi64;
+      uint32_t* keepq = a.far[fp ^ 1];
+      for (uint64_t base = gtid - lane; base < nfar; base += gthreads) {
+        const uint64_t i = base + lane;
+        bool to_near = false, keep = false;
+        uint32_t uu = 0, dd = 0;
+        if (i < nfar) {
+          uu = farq[i];
+          dd = a.dist[uu];
+          if (dd >= hi && dd < nhi) to_near = ell[(uint64_t)uu * D] != kNoArc;
+          else if (dd >= nhi) keep = true;
+          if (!keep) atomicAnd(&a.infar[uu >> 5], ~(1u << (uu & 31)));
+        }
+        worklists::publish(a.ring, to_near, make_uint4(uu, dd, 0u, 0u), &ctl->err);
+        warp_push(keep, uu, keepq, &ctl->far_count[fp ^ 1], a.n, &ctl->err);
+      }
+    }
+    bucket = nb;
+    fp ^= 1;
+    if (!grid_barrier(&ctl->bar, nblocks, &ctl->err, deadline)) return;
+  }
+  my_scanned = warp_sum(my_scanned);
+  my_relax = warp_sum(my_relax);
+  if (lane == 0) {
+    if (my_scanned) atomicAdd(&ctl->scanned, my_scanned);
+    if (my_relax) atomicAdd(&ctl->relax, my_relax);
+  }
+  if (gtid == 0) ctl->phases = P;
+}
+
 __global__ void sssp_reach_kernel(const uint32_t* __restrict__ dist, const uint64_t* __restrict__ offs,
                                   uint32_t n, unsigned long long* out) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -798,10 +1033,27 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
     GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(worklists::RingCtl), s));
     sssp_async_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     GB_CUDA(cudaGetLastError());
-    const void* kfn = reinterpret_cast<const void*>(&sssp_async<256>);
+    // sssp_async 2: fixed-width rows on a graph of degree <= 8
+    const uint32_t D = t.sssp_async == 2 && g->max_degree <= 8 ? (g->max_degree <= 4 ? 4u : 8u) : 0u;
+    const uint32_t* ell = nullptr;
+    if (D) {
+      if (!g->ell || g->ell_d != D) {
+        cudaFree(g->ell);
+        g->ell = nullptr;
+        g->ell_d = 0;
+        GB_CUDA(cudaMalloc(&g->ell, sizeof(uint32_t) * 2 * (uint64_t)n * D));
+        ell_build_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, g->col, g->w, n, D, g->ell);
+        GB_CUDA(cudaGetLastError());
+        g->ell_d = D;
+      }
+      ell = g->ell;
+    }
+    const void* kfn = D == 4   ? reinterpret_cast<const void*>(&sssp_async_ell<256, 4>)
+                      : D == 8 ? reinterpret_cast<const void*>(&sssp_async_ell<256, 8>)
+                               : reinterpret_cast<const void*>(&sssp_async<256>);
     const int grid = coop_grid(g, kfn, 256, 0, t.blocks_per_sm);
     if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
-    void* args[] = {&a};
+    void* args[] = {&a, &ell};
     KernelTimer kt(stats != nullptr, s);
     GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, 256, args, 0, s));
     kt.stop(s);

@@ -23,6 +23,19 @@ def star_graph(k):
     return HostCSR.from_edges(k + 1, [0] * k + list(range(1, k + 1)), list(range(1, k + 1)) + [0] * k)
 
 
+def grid8(rows, cols):
+    """rows x cols grid with the 8 king-move neighbours (degree <= 8)."""
+    s, d = [], []
+    for r in range(rows):
+        for c in range(cols):
+            for dr in (-1, 0, 1):
+                for dc in (-1, 0, 1):
+                    if (dr or dc) and 0 <= r + dr < rows and 0 <= c + dc < cols:
+                        s.append(r * cols + c)
+                        d.append((r + dr) * cols + c + dc)
+    return HostCSR.from_edges(rows * cols, s, d)
+
+
 def union(*gs):
     """Block-diagonal union of host graphs."""
     off = 0
@@ -173,17 +186,21 @@ def test_sssp_async_buckets_bit_exact(cuda_device, shift):
     (unreachable part), from several sources."""
     er = erdos_renyi(30000, 3.0, seed=9)
     cases = [(grid2d(120, 70), (0, 4321)), (er, (0, 12345)), (path_graph(2000), (0, 999)),
-             (union(grid2d(30, 30), path_graph(100)), (5, 950))]
+             (union(grid2d(30, 30), path_graph(100)), (5, 950)), (grid8(90, 60), (0, 2999))]
     for g, srcs in cases:
         assign_weights_u32(g, 1, 255, seed=int(g.n))
         assert g.degrees().max() <= 32
         with DeviceGraph(g, symmetric=True) as dg:
             for src in srcs:
                 want = oracle.sssp_dijkstra(g, src)
-                dg.set_tuning(local_depth=8, sssp_async=1)
-                got, st = dg.sssp(src, shift, stats=True)
-                assert (got == want).all(), f"async n={g.n} src={src}"
-                assert st["vertices_reached"] == int((want != INF).sum())
+                # 1: asynchronous buckets; 2: the same over fixed-width rows
+                # (degree <= 4 or <= 8; the Erdos-Renyi graph's degree is above 8, so it
+                # takes the plain asynchronous kernel)
+                for mode in (1, 2):
+                    dg.set_tuning(local_depth=8, sssp_async=mode)
+                    got, st = dg.sssp(src, shift, stats=True)
+                    assert (got == want).all(), f"async {mode} n={g.n} src={src}"
+                    assert st["vertices_reached"] == int((want != INF).sum())
                 dg.set_tuning(sssp_async=0)
                 assert (dg.sssp(src, shift) == want).all(), f"phase-synchronous n={g.n} src={src}"
 
@@ -195,14 +212,21 @@ def test_sssp_async_small_ring_and_blocks(cuda_device):
     assign_weights_u32(g, 1, 255, seed=77)
     want = oracle.sssp_dijkstra(g, 777)
     with DeviceGraph(g, symmetric=True) as dg:
-        dg.set_tuning(local_depth=4, blocks_per_sm=1, sssp_async=1)
-        assert (dg.sssp(777, 13) == want).all()
+        for mode in (1, 2):
+            dg.set_tuning(local_depth=4, blocks_per_sm=1, sssp_async=mode)
+            assert (dg.sssp(777, 13) == want).all()
+        # the rows carry the weights: new weights rebuild them
+        dg.assign_weights_u32(1, 255, 78)
+        g.w_u32 = None
+        assign_weights_u32(g, 1, 255, seed=78)
+        assert (dg.sssp(777, 13) == oracle.sssp_dijkstra(g, 777)).all()
     iso = union(path_graph(1), grid2d(10, 10))
     iso.w_u32 = np.ones(iso.m, np.uint32)
     with DeviceGraph(iso, symmetric=True) as dg:
-        dg.set_tuning(sssp_async=1)
-        got = dg.sssp(0, 13)
-        assert got[0] == 0 and (got[1:] == INF).all()
+        for mode in (1, 2):
+            dg.set_tuning(sssp_async=mode)
+            got = dg.sssp(0, 13)
+            assert got[0] == 0 and (got[1:] == INF).all()
 
 
 def test_sssp_local_queues_rmat(cuda_device):
