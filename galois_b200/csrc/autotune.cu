@@ -119,8 +119,10 @@ extern "C" int gb_autotune(gb_graph* g, const char* kernel, uint32_t src, const 
           t.local_depth = depth;
           t.sssp_async = 0;
           cands.push_back(t);
-          if (depth > 0) {  // asynchronous buckets (taken only when every vertex is light)
-            t.sssp_async = 1;
+          if (depth > 0) {  // asynchronous buckets (taken only when every vertex is light),
+            t.sssp_async = 1;  // then over fixed-width rows (degree <= 8)
+            cands.push_back(t);
+            t.sssp_async = 2;
             cands.push_back(t);
           }
         }

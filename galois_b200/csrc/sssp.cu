@@ -48,10 +48,14 @@
 // (gb_worklist.cuh); a bucket ends when the worklist's work count reaches
 // zero, and only the bucket transitions keep grid barriers -- the schedule
 // of the reference's barrier-free OBIM inside a bucket.  On the 4096^2 grid
-// it measured 42.5-44 ms against 40.8 ms for the phase-synchronous kernel
-// (more arcs re-relaxed, 9.7x against 6.7x the reached arcs, while the
-// ~8 K-hop dependent chain sets both times), so the phase-synchronous
-// kernel stays the default.
+// it measured 43.8 ms against 40.6 ms for the phase-synchronous kernel
+// (more arcs re-relaxed, 9.7x against 6.7x the reached arcs), so the
+// phase-synchronous kernel stays the default.  sssp_async_ell (tuning
+// sssp_async = 2, degree <= 8) carries each queued vertex's fixed-width row:
+// one memory round trip per hop, 0.69 against 1.45 us per hop on a path, but
+// a round covers 32 / D vertices instead of 32 and it re-relaxes more
+// (13.7x), so on the grid's wide wavefront it is slower (115 ms); the
+// autotuner may pick it for narrow, chain-like graphs.
 
 #include "device_common.cuh"
 #include "device_graph.cuh"

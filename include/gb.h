@@ -233,9 +233,13 @@ typedef struct gb_tuning {
   int local_depth;       /* SSSP: per-warp local-queue rounds per phase
                             (0 = library default, < 0 = off) */
   int sssp_async;        /* SSSP with local queues on a graph whose every
-                            vertex is light: > 0 = asynchronous buckets (no
-                            grid barrier inside a bucket), <= 0 = library
-                            default (a grid barrier after every phase) */
+                            vertex is light: 1 = asynchronous buckets (no
+                            grid barrier inside a bucket), 2 = the same over
+                            fixed-width rows when the degree is <= 8 (one
+                            memory round trip per hop: faster on narrow,
+                            chain-like graphs, slower on wide wavefronts),
+                            <= 0 = library default (a grid barrier after
+                            every phase) */
 } gb_tuning;
 int gb_graph_set_tuning(gb_graph* g, const gb_tuning* t);
 int gb_graph_get_tuning(const gb_graph* g, gb_tuning* t);
