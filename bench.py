@@ -1141,7 +1141,8 @@ def main() -> None:
                 with DeviceGraph(HostCSR(a, b, c), symmetric=g["symmetric"], device=dev) as dg:
                     job.device_call(dg, gi, host_out[gi])
 
-        e2e_step()
+        for _ in range(2):  # untimed: the first calls also fill the allocator cache and page in the buffers
+            e2e_step()
         ke = max(1, min(args.steps, 10))
         dist.barrier()
         t0 = time.perf_counter()
