@@ -145,6 +145,7 @@ SIGNATURES: dict[str, tuple] = {
     "gb_ppr_backward": (C.c_int, [_gp, C.c_uint32, _vp, _vp, _vp, C.c_float, C.c_float, C.c_uint32, _vp,
                                   _vp, _u32p, C.POINTER(Stats), _vp]),
     "gb_autotune": (C.c_int, [_gp, C.c_char_p, C.c_uint32, C.c_char_p, C.POINTER(Tuning), _vp]),
+    "gb_probe_bounded_waits": (C.c_int, [C.c_int, C.c_uint32, _vp]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

@@ -383,6 +383,14 @@ int gb_ppr_backward(gb_graph* g, uint32_t B, const float* x, const float* gx,
                     float* grad_teleport, float* grad_w, uint32_t* iters_out,
                     gb_stats* stats, void* stream);
 
+/* Failure detection check (no counterpart in the reference): runs one of the
+ * device waits the persistent kernels rely on -- which = 0: the software grid
+ * barrier with one CTA that never arrives; 1: a worklist ticket whose chunk is
+ * never published -- with a limit of limit_us microseconds (1 .. 2e6).  The
+ * wait gives up, the kernel returns, and the call returns GB_ERR_TIMEOUT;
+ * the context stays usable.  Synchronous on `stream`. */
+int gb_probe_bounded_waits(int which, uint32_t limit_us, void* stream);
+
 /* Autotuner: times candidate degree-bin thresholds, tile sizes, CTA shapes
  * and push/pull switch points for `kernel` ("bfs", "sssp", "cc", "pr") on this
  * graph, keeps the fastest in the handle, and (if cache_path is non-NULL)
