@@ -29,6 +29,7 @@ GB_CC_AFFOREST = 2
 GB_ORDER_NONE = 0
 GB_ORDER_DEGREE = 1
 GB_ORDER_DEGREE_UNSORTED = 2
+GB_ORDER_LOCALITY = 3
 GB_PR_PUSH_ASYNC = 0
 GB_PR_PUSH_SYNC = 1
 

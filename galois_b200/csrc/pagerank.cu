@@ -857,7 +857,8 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
     pr_pull_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     a.zero_from = g->perm ? g->zero_from : n;
     kfn = reinterpret_cast<const void*>(&pr_pull_persistent<kBlock, 2, 6>);
-    if (g->perm) {
+    // the flat sweep needs the degree order: heavy rows first, the light rows' arcs one range
+    if (g->perm && (g->order == GB_ORDER_DEGREE || g->order == GB_ORDER_DEGREE_UNSORTED)) {
       // degree-ordered: heavy rows are [0, nheavy), the light rows' arcs one
       // contiguous range swept flat
       st = light_run_table(g, sched, &a, s);

@@ -8,9 +8,19 @@
 // a few lines that stay in L1/L2.  The kernels are unchanged: they run on the
 // relabelled CSR, and the entry points translate sources in and results out.
 //
+// GB_ORDER_LOCALITY (no counterpart in the reference either) serves
+// bounded-degree, high-diameter graphs instead (grids, meshes, road-like
+// graphs): without coordinates it takes a vertex's BFS distances to two
+// far-apart landmarks as coordinates (landmark A: the vertex farthest from
+// vertex 0; B: farthest from A; C: farthest from both A and B -- on a grid,
+// three corners -- coordinates (d_A, d_C)) and numbers the vertices in the
+// Morton (Z) order of those coordinates, so that consecutive ids form compact
+// 2-D patches instead of long rows.
+//
 // Steps (all on the device, one stream):
 //   1. deg[v] = offs[v+1] - offs[v]; radix sort (deg desc, id) -> perm
 //      (new -> old, stable so equal degrees keep id order); iperm = inverse
+//      [locality: radix sort (Morton key, id) -> perm]
 //   2. new offsets = exclusive scan of the sorted degrees
 //   3. one warp per new row copies the old row with columns mapped through
 //      iperm (weights follow their arcs)
@@ -26,6 +36,10 @@
 #include "device_graph.cuh"
 
 namespace gb {
+
+int run_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats, cudaStream_t s, void* scratch,
+            size_t scratch_bytes);
+
 namespace {
 
 __global__ void degree_ids_kernel(const uint64_t* __restrict__ offs, uint32_t n, uint32_t* __restrict__ deg,
@@ -116,6 +130,60 @@ __global__ void label_out_kernel(const uint32_t* __restrict__ lab, const uint32_
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += stride)
     out[v] = minorig[lab[iperm[v]]];
+}
+
+// Largest reached level, ties to the smallest id: key = level << 32 | ~v.
+__global__ void far_vertex_kernel(const uint32_t* __restrict__ lv, const uint32_t* __restrict__ lv2, uint32_t n,
+                                  unsigned long long* best) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long mine = 0;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += stride) {
+    uint32_t d = lv[v];
+    if (d == kInf) continue;
+    if (lv2) {  // farthest from both: the smaller of the two distances
+      const uint32_t d2 = lv2[v];
+      if (d2 == kInf) continue;
+      d = min(d, d2);
+    }
+    const unsigned long long key = ((unsigned long long)d << 32) | (0xFFFFFFFFu - (uint32_t)v);
+    mine = key > mine ? key : mine;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(kFull, mine, o);
+    mine = other > mine ? other : mine;
+  }
+  if ((threadIdx.x & 31) == 0 && mine) atomicMax(best, mine);
+}
+
+__device__ __forceinline__ uint32_t spread16(uint32_t x) {  // bit i -> bit 2i
+  x &= 0xFFFFu;
+  x = (x | (x << 8)) & 0x00FF00FFu;
+  x = (x | (x << 4)) & 0x0F0F0F0Fu;
+  x = (x | (x << 2)) & 0x33333333u;
+  x = (x | (x << 1)) & 0x55555555u;
+  return x;
+}
+
+// Morton key of (dx, dy) >> shift per vertex; unreached vertices go last.
+__global__ void morton_kernel(const uint32_t* __restrict__ dx, const uint32_t* __restrict__ dy, uint32_t n,
+                              uint32_t shift, uint32_t* __restrict__ key, uint32_t* __restrict__ ids) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += stride) {
+    const uint32_t x = dx[v], y = dy[v];
+    key[v] = (x == kInf || y == kInf) ? 0xFFFFFFFFu : (spread16(x >> shift) | (spread16(y >> shift) << 1));
+    ids[v] = (uint32_t)v;
+  }
+}
+
+__global__ void gather_deg_kernel(const uint64_t* __restrict__ offs, const uint32_t* __restrict__ perm, uint32_t n,
+                                  uint32_t* __restrict__ deg_sorted) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t v = perm[i];
+    const uint64_t d = offs[v + 1] - offs[v];
+    deg_sorted[i] = d > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)d;
+  }
 }
 
 int blocks_for(const gb_graph* g, uint64_t work) {
@@ -211,7 +279,7 @@ int reorder_graph(gb_graph* g, int order, cudaStream_t s) {
     if (g->perm) GB_FAIL(GB_ERR_UNSUPPORTED, "gb_graph_reorder: a relabelled graph cannot be restored");
     return GB_OK;
   }
-  if (order != GB_ORDER_DEGREE && order != GB_ORDER_DEGREE_UNSORTED)
+  if (order != GB_ORDER_DEGREE && order != GB_ORDER_DEGREE_UNSORTED && order != GB_ORDER_LOCALITY)
     GB_FAIL(GB_ERR_ARG, "gb_graph_reorder: unknown order %d", order);
   if (g->perm) {
     if (g->order == order) return GB_OK;
@@ -219,7 +287,8 @@ int reorder_graph(gb_graph* g, int order, cudaStream_t s) {
   }
   const uint32_t n = g->n;
   const uint64_t m = g->m;
-  const bool sort_rows = order == GB_ORDER_DEGREE && m < (1ull << 31);
+  const bool sort_rows = order != GB_ORDER_DEGREE_UNSORTED && m < (1ull << 31);
+  const bool locality = order == GB_ORDER_LOCALITY;
   const bool weighted = g->w || g->wf;
 
   uint32_t *deg = nullptr, *deg2 = nullptr, *ids = nullptr, *perm = nullptr, *iperm = nullptr;
@@ -230,7 +299,15 @@ int reorder_graph(gb_graph* g, int order, cudaStream_t s) {
   uint32_t* h_iperm = nullptr;
   void* tmp = nullptr;
   size_t tmp_bytes = 0;
+  uint32_t *da = nullptr, *db = nullptr, *dc = nullptr;  // locality: landmark distances
+  unsigned long long* best = nullptr;
   auto cleanup = [&](bool keep_new) {
+    cudaFree(da);
+    cudaFree(db);
+    cudaFree(dc);
+    cudaFree(best);
+    da = db = dc = nullptr;
+    best = nullptr;
     cudaFree(deg);
     cudaFree(deg2);
     cudaFree(ids);
@@ -274,20 +351,74 @@ int reorder_graph(gb_graph* g, int order, cudaStream_t s) {
     GB_FAIL(GB_ERR_OOM, "gb_graph_reorder: host allocation failed");
   }
 
-  // 1. degree-descending permutation
-  degree_ids_kernel<<<blocks_for(g, n), 256, 0, s>>>(g->offs, n, deg, ids);
-  GB_TRY(cudaMemsetAsync(deg2 + n, 0, sizeof(uint32_t), s));
-  int end_bit = 1;
-  while (end_bit < 32 && (1ull << end_bit) <= (uint64_t)g->max_degree) ++end_bit;
-  GB_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, deg, deg2, ids, perm, (int64_t)n, 0, end_bit, s));
-  GB_TRY(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 16)));
-  GB_TRY(cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, deg, deg2, ids, perm, (int64_t)n, 0, end_bit, s));
-  invert_kernel<<<blocks_for(g, n), 256, 0, s>>>(perm, n, iperm);
-  uint32_t* zf = reinterpret_cast<uint32_t*>(ids);  // ids is free after the sort
-  GB_TRY(cudaMemcpyAsync(zf, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  first_zero_kernel<<<blocks_for(g, n), 256, 0, s>>>(deg2, n, zf);
   uint32_t zero_from = n;
-  GB_TRY(cudaMemcpyAsync(&zero_from, zf, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GB_TRY(cudaMemsetAsync(deg2 + n, 0, sizeof(uint32_t), s));
+  if (!locality) {
+    // 1. degree-descending permutation
+    degree_ids_kernel<<<blocks_for(g, n), 256, 0, s>>>(g->offs, n, deg, ids);
+    int end_bit = 1;
+    while (end_bit < 32 && (1ull << end_bit) <= (uint64_t)g->max_degree) ++end_bit;
+    GB_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, deg, deg2, ids, perm, (int64_t)n, 0, end_bit,
+                                                     s));
+    GB_TRY(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 16)));
+    GB_TRY(cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, deg, deg2, ids, perm, (int64_t)n, 0, end_bit, s));
+    uint32_t* zf = reinterpret_cast<uint32_t*>(ids);  // ids is free after the sort
+    GB_TRY(cudaMemcpyAsync(zf, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    first_zero_kernel<<<blocks_for(g, n), 256, 0, s>>>(deg2, n, zf);
+    GB_TRY(cudaMemcpyAsync(&zero_from, zf, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  } else {
+    // 1. Morton order of the distances to two far-apart landmarks
+    GB_TRY(cudaMalloc(&da, sizeof(uint32_t) * n));
+    GB_TRY(cudaMalloc(&db, sizeof(uint32_t) * n));
+    GB_TRY(cudaMalloc(&dc, sizeof(uint32_t) * n));
+    GB_TRY(cudaMalloc(&best, sizeof(unsigned long long)));
+    // the farthest reached vertex from `from` (optionally: from both)
+    auto farthest = [&](const uint32_t* lv, const uint32_t* lv2, uint32_t* out) -> int {
+      cudaError_t e = cudaMemsetAsync(best, 0, sizeof(unsigned long long), s);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+      far_vertex_kernel<<<blocks_for(g, n), 256, 0, s>>>(lv, lv2, n, best);
+      unsigned long long h = 0;
+      e = cudaMemcpyAsync(&h, best, sizeof(h), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return cuda_fail(e, "landmark search");
+      *out = h ? 0xFFFFFFFFu - (uint32_t)(h & 0xFFFFFFFFull) : 0u;
+      return GB_OK;
+    };
+    uint32_t a0 = 0, la = 0, lb = 0, lc = 0;
+    int lst = run_bfs(g, a0, da, nullptr, s, nullptr, 0);
+    if (lst == GB_OK) lst = farthest(da, nullptr, &la);
+    if (lst == GB_OK) lst = run_bfs(g, la, da, nullptr, s, nullptr, 0);
+    if (lst == GB_OK) lst = farthest(da, nullptr, &lb);
+    if (lst == GB_OK) lst = run_bfs(g, lb, db, nullptr, s, nullptr, 0);
+    if (lst == GB_OK) lst = farthest(da, db, &lc);
+    if (lst == GB_OK) lst = run_bfs(g, lc, dc, nullptr, s, nullptr, 0);
+    if (lst != GB_OK) {
+      cleanup(false);
+      return lst;
+    }
+    // the largest coordinate decides how far the keys are shifted to fit 16 bits
+    uint32_t ma = 0, mc = 0;
+    {
+      int fst = farthest(da, nullptr, &ma);
+      if (fst == GB_OK) fst = farthest(dc, nullptr, &mc);
+      if (fst != GB_OK) {
+        cleanup(false);
+        return fst;
+      }
+    }
+    uint32_t hmax[2] = {0, 0};
+    GB_TRY(cudaMemcpyAsync(&hmax[0], da + ma, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GB_TRY(cudaMemcpyAsync(&hmax[1], dc + mc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GB_TRY(cudaStreamSynchronize(s));
+    uint32_t shift = 0;
+    while ((std::max(hmax[0], hmax[1]) >> shift) > 0xFFFFu) ++shift;
+    morton_kernel<<<blocks_for(g, n), 256, 0, s>>>(da, dc, n, shift, deg, ids);
+    GB_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, deg, db, ids, perm, (int64_t)n, 0, 32, s));
+    GB_TRY(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 16)));
+    GB_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, deg, db, ids, perm, (int64_t)n, 0, 32, s));
+    gather_deg_kernel<<<blocks_for(g, n), 256, 0, s>>>(g->offs, perm, n, deg2);
+  }
+  invert_kernel<<<blocks_for(g, n), 256, 0, s>>>(perm, n, iperm);
 
   // 2. new offsets
   {

@@ -200,6 +200,12 @@ int gb_graph_assign_weights_f32(gb_graph* g, uint64_t seed, void* stream);
 #define GB_ORDER_NONE 0
 #define GB_ORDER_DEGREE 1
 #define GB_ORDER_DEGREE_UNSORTED 2
+/* GB_ORDER_LOCALITY: for bounded-degree, high-diameter graphs (grids, meshes,
+ * road-like graphs).  Vertices are numbered in the Morton order of their BFS
+ * distances to two far-apart landmark vertices (found by BFS: the vertex
+ * farthest from vertex 0, the one farthest from it, and the one farthest
+ * from both), so consecutive ids form compact 2-D patches; rows are sorted. */
+#define GB_ORDER_LOCALITY 3
 int gb_graph_reorder(gb_graph* g, int order, void* stream);
 /* Device permutation of a reordered graph: new_to_old[internal id] =
  * original id, old_to_new the inverse; both NULL if not reordered. */

@@ -1,7 +1,8 @@
-"""Degree-ordered relabelling (gb_graph_reorder): every algorithm keeps taking
-and returning original vertex ids, so the results match the oracle exactly
-(BFS/SSSP/CC) or within the stated tolerance (PageRank, BC), for host and
-device outputs, sorted and unsorted rows, symmetric and directed graphs."""
+"""Relabelling (gb_graph_reorder: degree order, and the locality order of
+landmark distances): every algorithm keeps taking and returning original
+vertex ids, so the results match the oracle exactly (BFS/SSSP/CC) or within
+the stated tolerance (PageRank, BC), for host and device outputs, sorted and
+unsorted rows, symmetric and directed graphs."""
 import numpy as np
 import pytest
 import torch
@@ -11,6 +12,7 @@ from galois_b200 import (GB_CC_AFFOREST, GB_CC_LABELPROP, GB_CC_UNIONFIND, GB_OR
                          GB_ORDER_DEGREE_UNSORTED, GB_ORDER_NONE, DeviceGraph, GbError, HostCSR,
                          assign_weights_f32, assign_weights_u32, grid2d, rmat)
 from galois_b200 import _lib
+from galois_b200._lib import GB_ORDER_LOCALITY
 from galois_b200.graph import pack_graphs
 
 pytestmark = pytest.mark.gpu
@@ -165,3 +167,54 @@ def test_autotune_on_reordered(cuda_device, tmp_path):
     with DeviceGraph(g, symmetric=True, reorder=GB_ORDER_DEGREE) as dg:
         dg.autotune("bfs", src, str(tmp_path / "tune.jsonl"))
         assert (dg.bfs(src) == oracle.bfs_serial(g, src)).all()
+
+
+def _perm_host(dg):
+    """new_to_old of a relabelled graph, copied to the host."""
+    ptr = dg.permutation()["new_to_old"]
+
+    class _View:
+        def __init__(self):
+            self.__cuda_array_interface__ = {"shape": (dg.n,), "typestr": "<i4", "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_View(), device="cuda").cpu().numpy().view(np.uint32)
+
+
+def test_locality_order_all_algorithms(cuda_device):
+    """GB_ORDER_LOCALITY on a grid with a detached path (a second component,
+    out of the landmarks' reach) and on an RMAT graph: BFS, SSSP (both
+    kernels), CC, PageRank pull and residual push in original ids, and the
+    permutation a bijection that keeps grid neighbours close."""
+    grid = grid2d(60, 70)
+    path_s = list(range(4199 + 1, 4199 + 30)) + list(range(4199 + 2, 4199 + 31))
+    path_d = list(range(4199 + 2, 4199 + 31)) + list(range(4199 + 1, 4199 + 30))
+    ends = np.concatenate([grid.end_offs, np.full(31, grid.m, np.uint64)])
+    g = HostCSR(ends, grid.col)
+    extra = HostCSR.from_edges(g.n, path_s, path_d)
+    s_all = np.concatenate([np.repeat(np.arange(g.n), g.degrees()), np.repeat(np.arange(g.n), extra.degrees())])
+    d_all = np.concatenate([g.col, extra.col])
+    g = HostCSR.from_edges(g.n, s_all, d_all)
+    assign_weights_u32(g, 1, 255, seed=11)
+    r, _ = rmat(12, 8, seed=13)
+    assign_weights_u32(r, 1, 255, seed=13)
+    for h in (g, r):
+        srcs = [0, int(np.argmax(h.degrees()))]
+        with DeviceGraph(h, symmetric=True, reorder=GB_ORDER_LOCALITY) as dg:
+            new_to_old = _perm_host(dg)
+            assert np.array_equal(np.sort(new_to_old), np.arange(h.n))
+            for src in srcs:
+                assert (dg.bfs(src) == oracle.bfs_serial(h, src)).all()
+                want = oracle.sssp_dijkstra(h, src)
+                for mode in (0, 1):
+                    dg.set_tuning(sssp_async=mode)
+                    assert (dg.sssp(src, 13) == want).all(), (h.n, src, mode)
+            assert (dg.cc(GB_CC_LABELPROP) == oracle.cc_union_find(h)).all()
+            want_pr, it64 = oracle.pr_pull_topo_f64(h, 0.85, 1e-6, 1000)
+            got_pr, st = dg.pagerank_pull(0.85, 1e-6, 1000, stats=True)
+            assert np.abs(got_pr - want_pr).max() < 1e-5 and abs(st["iterations"] - it64) <= 2
+    # on the grid, ids that are consecutive in the new order are close on the grid
+    with DeviceGraph(grid, symmetric=True, reorder=GB_ORDER_LOCALITY) as dg:
+        old = _perm_host(dg).astype(np.int64)
+    rows, cols = old // 70, old % 70
+    hop = np.abs(np.diff(rows)) + np.abs(np.diff(cols))
+    assert np.median(hop) <= 2
