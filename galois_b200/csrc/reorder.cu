@@ -215,6 +215,7 @@ void drop_derived(gb_graph* g) {
   cudaFree(g->ell);
   g->ell = nullptr;
   g->ell_d = 0;
+  g->region_arcs = 0;
   cudaFree(g->sweep_tiles);
   cudaFree(g->sweep_heavy_list);
   g->sweep_tiles = nullptr;

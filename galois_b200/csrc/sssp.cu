@@ -91,6 +91,7 @@ struct SsspCtl {
   uint32_t pad1;
   unsigned long long scanned;
   unsigned long long relax;
+  unsigned long long local_rounds;  // region kernel: shared-memory rounds over all visits
 };
 
 struct SsspArgs {
@@ -913,6 +914,428 @@ __global__ void __launch_bounds__(BLOCK) sssp_async_ell(SsspArgs a, const uint32
   if (gtid == 0) ctl->phases = P;
 }
 
+// ---- regions in shared memory (bounded-degree graphs numbered by locality) ---
+// On a graph numbered so that consecutive ids form compact patches
+// (GB_ORDER_LOCALITY), the vertices [r * kRegion, (r + 1) * kRegion) form
+// region r and most arcs stay inside their region.  A CTA takes one queued
+// region at a time, loads its distances, row offsets and arcs into shared
+// memory and relaxes to a local fixed point inside the current bucket: a hop
+// inside the region is a shared-memory atomic and a CTA barrier, not a global
+// round trip.  An arc that leaves the region lowers the global distance and
+// then either marks the target pending (one bit per vertex) and queues the
+// target's region, or files the target in the far pile.  Global distances
+// stay authoritative: the region writes its lowered distances back with
+// atomicMin, and pending bits set while it ran queue it again when it is
+// released.  Regions travel through the device worklist ring
+// (gb_worklist.cuh) as single ids, at most once each (a queued flag per
+// region); a bucket ends when no region is queued and no CTA holds one.
+
+constexpr uint32_t kRegion = 4096;       // vertices per region (a multiple of 32)
+constexpr uint32_t kRegionArcs = 16384;  // arcs a region may hold in shared memory
+constexpr uint32_t kRegionOut = 2048;    // outbox: relaxations of arcs leaving the region
+constexpr int kRegionBlock = 512;
+
+struct RegionArgs {
+  uint32_t* pend;  // bitmap: vertex lowered from outside its region, to be expanded
+  uint32_t* rq;    // per region: queued or being processed (1) or not (0)
+  uint32_t nregions;
+};
+
+constexpr size_t region_smem_bytes() {
+  return sizeof(uint32_t) * kRegion              // distances
+         + sizeof(uint32_t) * (kRegion + 4)      // local row offsets
+         + 2 * sizeof(uint32_t) * kRegionArcs    // columns, weights
+         + 2 * sizeof(uint16_t) * kRegion        // the two round worklists
+         + 2 * sizeof(uint32_t) * (kRegion / 32) // in-worklist bitmap, pending words taken
+         + sizeof(uint2) * kRegionOut;           // outbox
+}
+
+// Largest arc count of any region (host check that regions fit).
+__global__ void region_arcs_kernel(const uint64_t* __restrict__ offs, uint32_t n, uint32_t nregions,
+                                   unsigned long long* max_arcs) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long mine = 0;
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < nregions; r += stride) {
+    const uint64_t b = r * kRegion, e = b + kRegion < (uint64_t)n ? b + kRegion : (uint64_t)n;
+    mine = max(mine, (unsigned long long)(offs[e] - offs[b]));
+  }
+  for (int o = 16; o > 0; o >>= 1) mine = max(mine, __shfl_xor_sync(kFull, mine, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(max_arcs, mine);
+}
+
+__global__ void sssp_region_init(SsspArgs a, RegionArgs ra) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t words = (a.n + 31) >> 5;
+  for (uint64_t v = tid; v < a.n; v += stride) a.dist[v] = (v == a.src) ? 0u : kInf;
+  for (uint64_t w = tid; w < words; w += stride) {
+    a.infar[w] = 0;
+    ra.pend[w] = (w == (a.src >> 5)) ? (1u << (a.src & 31)) : 0u;
+  }
+  const uint32_t r0 = a.src / kRegion;
+  for (uint64_t r = tid; r < ra.nregions; r += stride) ra.rq[r] = (r == r0) ? 1u : 0u;
+  for (uint64_t i = tid; i <= a.ring.mask; i += stride) {
+    if (i == 0) {  // the source's region, published as the chunk of position 0 (counted in work)
+      a.ring.ent[0] = make_uint4(r0, 0u, 0u, 0u);
+      a.ring.cnt[0] = 1;
+      a.ring.seq[0] = 1;
+      a.ring.rc->tail = 1;
+      a.ring.rc->work = 1;
+    } else {
+      a.ring.seq[i] = i;
+    }
+  }
+}
+
+// u (outside the caller's region) was lowered to a distance inside the
+// bucket: mark it pending and queue its region unless it is queued.  The
+// fences order distance -> pending bit -> queued flag against the region's
+// release, which clears the flag and then reads the pending bits.
+__device__ __forceinline__ void region_touch(const SsspArgs& a, const RegionArgs& ra, uint32_t u, int* err) {
+  __threadfence();
+  atomicOr(&ra.pend[u >> 5], 1u << (u & 31));
+  __threadfence();
+  const uint32_t rg = u / kRegion;
+  if (*reinterpret_cast<volatile uint32_t*>(&ra.rq[rg]) == 0u && atomicCAS(&ra.rq[rg], 0u, 1u) == 0u)
+    worklists::publish_one(a.ring, make_uint4(rg, 0u, 0u, 0u), err);
+}
+
+// File u (lowered to a distance beyond the bucket) in the far pile once.
+__device__ __forceinline__ void far_file(const SsspArgs& a, uint32_t* farq, uint32_t* count, uint32_t u, int* err) {
+  const uint32_t bit = 1u << (u & 31);
+  if (!(__ldcg(a.infar + (u >> 5)) & bit) && !(atomicOr(&a.infar[u >> 5], bit) & bit)) {
+    const uint32_t pos = atomicAdd(count, 1u);
+    if (pos < a.n) farq[pos] = u;
+    else raise_err(err, kDevOverflow);
+  }
+}
+
+// Load a region into shared memory with 16-byte loads: its distances (base
+// is a multiple of kRegion, so 16-byte aligned), its nv + 1 offsets relative
+// to o0, and its na arcs from o0 (any alignment: the unaligned head and tail
+// are loaded one by one).  Only elements inside the arrays are read.
+__device__ __forceinline__ void region_load(const SsspArgs& a, uint32_t base, uint32_t nv, uint64_t o0, uint32_t na,
+                                            uint32_t* s_dist, uint32_t* s_loff, uint32_t* s_col, uint32_t* s_w) {
+  const uint32_t tid = threadIdx.x;
+  const uint4* d4 = reinterpret_cast<const uint4*>(a.dist + base);
+#pragma unroll 4
+  for (uint32_t q = tid; q < nv / 4; q += kRegionBlock) reinterpret_cast<uint4*>(s_dist)[q] = __ldcg(d4 + q);
+  for (uint32_t i = (nv & ~3u) + tid; i < nv; i += kRegionBlock) s_dist[i] = __ldcg(a.dist + base + i);
+  const ulonglong2* o2 = reinterpret_cast<const ulonglong2*>(a.offs + base);
+  const uint32_t npairs = (nv + 1) / 2;  // offsets [0, 2 * npairs) lie within [0, nv]
+#pragma unroll 4
+  for (uint32_t q = tid; q < npairs; q += kRegionBlock) {
+    const ulonglong2 x = ldg(o2 + q);
+    s_loff[2 * q] = (uint32_t)(x.x - o0);
+    s_loff[2 * q + 1] = (uint32_t)(x.y - o0);
+  }
+  if (tid == 0 && 2 * npairs == nv) s_loff[nv] = (uint32_t)(ldg(a.offs + base + nv) - o0);
+  // arcs: [o0, q0 * 4) and [q1 * 4, o0 + na) one by one, [q0, q1) as 16-byte words
+  const uint64_t e = o0 + na;
+  const uint64_t q0 = (o0 + 3) / 4, q1 = e / 4;
+  if (q0 < q1) {
+    const uint4* c4 = reinterpret_cast<const uint4*>(a.col);
+    const uint4* w4 = reinterpret_cast<const uint4*>(a.w);
+    const uint32_t nq = (uint32_t)(q1 - q0);
+    const uint32_t off = (uint32_t)(q0 * 4 - o0);
+#pragma unroll 4
+    for (uint32_t q = tid; q < nq; q += kRegionBlock) {
+      const uint4 c = ldg(c4 + q0 + q), w = ldg(w4 + q0 + q);
+      const uint32_t j = off + 4 * q;
+      s_col[j] = c.x, s_col[j + 1] = c.y, s_col[j + 2] = c.z, s_col[j + 3] = c.w;
+      s_w[j] = w.x, s_w[j + 1] = w.y, s_w[j + 2] = w.z, s_w[j + 3] = w.w;
+    }
+    for (uint32_t t = tid; t < off; t += kRegionBlock) {
+      s_col[t] = ldg(a.col + o0 + t);
+      s_w[t] = ldg(a.w + o0 + t);
+    }
+    for (uint64_t g = q1 * 4 + tid; g < e; g += kRegionBlock) {
+      s_col[g - o0] = ldg(a.col + g);
+      s_w[g - o0] = ldg(a.w + g);
+    }
+  } else {
+    for (uint32_t t = tid; t < na; t += kRegionBlock) {
+      s_col[t] = ldg(a.col + o0 + t);
+      s_w[t] = ldg(a.w + o0 + t);
+    }
+  }
+}
+
+// Needs every region's arcs to fit (at most kRegionArcs; checked on the host).
+__global__ void __launch_bounds__(kRegionBlock, 1) sssp_region(SsspArgs a, RegionArgs ra) {
+  static_assert(worklists::kErrTimeout == kDevTimeout && worklists::kErrOverflow == kDevOverflow,
+                "the worklist raises the library's device error codes");
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  uint32_t* s_dist = reinterpret_cast<uint32_t*>(s_raw);
+  uint32_t* s_loff = s_dist + kRegion;
+  uint32_t* s_col = s_loff + kRegion + 4;
+  uint32_t* s_w = s_col + kRegionArcs;
+  uint2* s_out = reinterpret_cast<uint2*>(s_w + kRegionArcs);
+  uint32_t* s_inq = reinterpret_cast<uint32_t*>(s_out + kRegionOut);
+  uint32_t* s_pw = s_inq + kRegion / 32;
+  uint16_t* s_wl = reinterpret_cast<uint16_t*>(s_pw + kRegion / 32);  // [2][kRegion]
+  __shared__ uint32_t s_region, s_go, s_n[3], s_nout;
+  const uint32_t flush_every = a.local_depth > 0 ? (uint32_t)a.local_depth : 8u;
+  SsspCtl* ctl = a.ctl;
+  worklists::RingCtl* rc = a.ring.rc;
+  const uint32_t tid = threadIdx.x, lane = lane_id();
+  const uint64_t deadline = kernel_deadline();
+  const uint64_t gtid = blockIdx.x * (uint64_t)kRegionBlock + tid;
+  const uint64_t gthreads = (uint64_t)gridDim.x * kRegionBlock;
+  unsigned long long my_scanned = 0, my_relax = 0, my_rounds = 0;
+  uint32_t bucket = 0;
+  int fp = 0;
+  uint32_t P = 0;
+  bool busy = false;  // thread 0: this CTA holds one count of rc->work
+  for (;;) {
+    if (P >= a.max_phases) {
+      if (gtid == 0) raise_err(&ctl->err, kDevMaxRounds);
+      break;
+    }
+    const uint64_t hi64 = ((uint64_t)bucket + 1) << a.shift;
+    const uint32_t hi = hi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)hi64;
+    uint32_t* farq = a.far[fp];
+    uint32_t* far_count = &ctl->far_count[fp];
+    // ---- the bucket's regions, no grid barrier ---------------------------------
+    for (;;) {
+      if (tid == 0) {
+        if (busy) atomicSub(&rc->work, 1);
+        busy = false;
+        const unsigned long long p = atomicAdd(&rc->head, 1ull);
+        const int got = worklists::wait_chunk(a.ring, p, &ctl->err, deadline);
+        s_go = got > 0 ? 1u : 0u;
+        if (got > 0) {
+          busy = true;  // the chunk's count is now this CTA's
+          const unsigned long long cs = p & a.ring.mask;
+          s_region = __ldcg(&a.ring.ent[cs * 32].x);
+          worklists::st_release(a.ring.seq + cs, p + a.ring.mask + 1);
+        }
+      }
+      __syncthreads();
+      if (!s_go) break;  // the bucket is done (or an error was raised)
+      const uint32_t r = s_region;
+      const uint32_t base = r * kRegion;
+      const uint32_t nv = min(kRegion, a.n - base);
+      const uint32_t nw = (nv + 31) >> 5;
+      const uint64_t o0 = ldg(a.offs + base);
+      const uint32_t na = (uint32_t)(ldg(a.offs + base + nv) - o0);
+      if (tid == 0) s_n[0] = s_n[1] = s_n[2] = s_nout = 0;
+      __syncthreads();
+      // the pending vertices start the worklist; they are taken before the
+      // distances are read, so a lowering after this point sets its bit again
+      for (uint32_t j = tid; j < kRegion / 32; j += kRegionBlock) {
+        uint32_t bits = j < nw ? atomicExch(&ra.pend[(base >> 5) + j], 0u) : 0u;
+        s_inq[j] = bits;
+        if (bits) {
+          const uint32_t pos = atomicAdd(&s_n[0], (uint32_t)__popc(bits));
+          for (uint32_t k = 0; bits; ++k, bits &= bits - 1) s_wl[pos + k] = (uint16_t)(j * 32 + __ffs(bits) - 1);
+        }
+      }
+      __threadfence();
+      __syncthreads();
+      region_load(a, base, nv, o0, na, s_dist, s_loff, s_col, s_w);
+      __syncthreads();
+      // local rounds: every listed vertex's arcs, in shared memory inside the
+      // region; an arc that leaves the region goes to the outbox, which is
+      // flushed to the global distances every `flush_every` rounds (and when
+      // the round list runs dry or the outbox fills), so no round waits on a
+      // global atomic; each flush also takes in this region's vertices
+      // lowered from outside meanwhile
+      // Round k relaxes list k & 1 (count s_n[k % 3]) into list (k + 1) & 1
+      // (count s_n[(k + 1) % 3]) and zeroes s_n[(k + 2) % 3], so one CTA
+      // barrier per round suffices.  Four lanes share a list entry, one arc
+      // each; appends are aggregated per warp.
+      const uint32_t lanemask_lt = (1u << lane) - 1u;
+      uint32_t k = 0, since = 0;
+      for (;; ++k) {
+        const uint32_t cnt = s_n[k % 3];
+        const uint16_t* wl = s_wl + (k & 1) * kRegion;
+        uint16_t* wl_next = s_wl + ((k + 1) & 1) * kRegion;
+        uint32_t* n_next = &s_n[(k + 1) % 3];
+        if (tid == 0) s_n[(k + 2) % 3] = 0;
+        for (uint32_t i0 = (tid >> 5) * 8; i0 < cnt; i0 += kRegionBlock / 4) {  // warp-uniform
+          const uint32_t i = i0 + (lane >> 2), sub = lane & 3u;
+          const bool has = i < cnt;
+          const uint32_t v = has ? (uint32_t)wl[i] : 0u;
+          uint32_t d = hi;
+          if (has && sub == 0) {
+            atomicAnd(&s_inq[v >> 5], ~(1u << (v & 31)));
+            __threadfence_block();
+            d = *reinterpret_cast<volatile uint32_t*>(&s_dist[v]);
+          }
+          d = __shfl_sync(kFull, d, lane & ~3u);
+          const bool live = has && d < hi;
+          uint32_t j = live ? s_loff[v] + sub : 0u;
+          const uint32_t e1 = live ? s_loff[v + 1] : 0u;
+          while (__any_sync(kFull, j < e1)) {
+            bool to_next = false, to_out = false;
+            uint32_t u = 0, lu = 0, nd = 0;
+            if (j < e1) {
+              u = s_col[j];
+              nd = d + s_w[j];
+              j += 4;
+              ++my_scanned;
+              lu = u - base;
+              if (lu < nv) {
+                if (nd < *reinterpret_cast<volatile uint32_t*>(&s_dist[lu]) && nd < atomicMin(&s_dist[lu], nd)) {
+                  ++my_relax;
+                  const uint32_t bit = 1u << (lu & 31);
+                  to_next = nd < hi && !(atomicOr(&s_inq[lu >> 5], bit) & bit);
+                }
+              } else {
+                to_out = true;
+              }
+            }
+            const unsigned mn = __ballot_sync(kFull, to_next);
+            if (mn) {
+              const int lead = __ffs(mn) - 1;
+              uint32_t b0 = 0;
+              if ((int)lane == lead) b0 = atomicAdd(n_next, (uint32_t)__popc(mn));
+              b0 = __shfl_sync(kFull, b0, lead);
+              if (to_next) wl_next[b0 + __popc(mn & lanemask_lt)] = (uint16_t)lu;
+            }
+            const unsigned mo = __ballot_sync(kFull, to_out);
+            if (mo) {
+              const int lead = __ffs(mo) - 1;
+              uint32_t b0 = 0;
+              if ((int)lane == lead) b0 = atomicAdd(&s_nout, (uint32_t)__popc(mo));
+              b0 = __shfl_sync(kFull, b0, lead);
+              const uint32_t pos = b0 + __popc(mo & lanemask_lt);
+              if (to_out) {
+                if (pos < kRegionOut) {
+                  s_out[pos] = make_uint2(u, nd);
+                } else if (nd < __ldcg(a.dist + u) && nd < atomicMin(&a.dist[u], nd)) {  // outbox full
+                  ++my_relax;
+                  if (nd < hi) region_touch(a, ra, u, &ctl->err);
+                  else far_file(a, farq, far_count, u, &ctl->err);
+                }
+              }
+            }
+          }
+        }
+        __syncthreads();
+        // uniform: s_n[(k + 1) % 3] and s_nout change only after the next
+        // barrier (round k + 1 appends to s_n[(k + 2) % 3])
+        if (*n_next != 0 && ++since < flush_every) continue;
+        since = 0;
+        const uint32_t no = min(s_nout, kRegionOut);
+        for (uint32_t i = tid; i < no; i += kRegionBlock) {
+          const uint2 o = s_out[i];
+          if (o.y < atomicMin(&a.dist[o.x], o.y)) {
+            ++my_relax;
+            if (o.y < hi) region_touch(a, ra, o.x, &ctl->err);
+            else far_file(a, farq, far_count, o.x, &ctl->err);
+          }
+        }
+        // take the pending bits before reading the distances they announce
+        for (uint32_t j = tid; j < nw; j += kRegionBlock) {
+          uint32_t bits = *reinterpret_cast<volatile uint32_t*>(&ra.pend[(base >> 5) + j]);
+          if (bits) bits = atomicExch(&ra.pend[(base >> 5) + j], 0u);
+          s_pw[j] = bits;
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) s_nout = 0;
+        for (uint32_t i = tid; i < nv; i += kRegionBlock) {
+          if (!((s_pw[i >> 5] >> (i & 31)) & 1u)) continue;
+          // a bit asks for an expansion at the global distance: also when
+          // it equals the local one (the distance may have been read at the
+          // visit's start before its bit was set); a smaller local distance
+          // was lowered here and is expanded already
+          const uint32_t gd = __ldcg(a.dist + base + i);
+          if (gd <= s_dist[i]) {
+            s_dist[i] = gd;  // no relaxation runs during the flush
+            const uint32_t bit = 1u << (i & 31);
+            if (gd < hi && !(atomicOr(&s_inq[i >> 5], bit) & bit)) wl_next[atomicAdd(n_next, 1u)] = (uint16_t)i;
+          }
+        }
+        __syncthreads();
+        if (*n_next == 0) break;
+      }
+      if (tid == 0) my_rounds += k + 1;
+      // write the lowered distances back; those beyond the bucket join the far pile
+      for (uint32_t i = tid; i < nv; i += kRegionBlock) {
+        const uint32_t d = s_dist[i];
+        if (d < __ldcg(a.dist + base + i) && d < atomicMin(&a.dist[base + i], d) && d >= hi)
+          far_file(a, farq, far_count, base + i, &ctl->err);
+      }
+      __syncthreads();
+      // release: vertices lowered from outside meanwhile queue the region again
+      if (tid == 0) {
+        __threadfence();
+        atomicExch(&ra.rq[r], 0u);
+        __threadfence();
+      }
+      __syncthreads();
+      if (tid < 32) {
+        __threadfence();
+        bool any = false;
+        for (uint32_t j = tid; j < nw; j += 32)
+          any |= *reinterpret_cast<volatile uint32_t*>(&ra.pend[(base >> 5) + j]) != 0u;
+        if (__any_sync(kFull, any) && tid == 0 && atomicCAS(&ra.rq[r], 0u, 1u) == 0u)
+          worklists::publish_one(a.ring, make_uint4(r, 0u, 0u, 0u), &ctl->err);
+      }
+      __syncthreads();
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    // ---- bucket transition ---------------------------------------------------------
+    const uint32_t nfar = min(ctl->far_count[fp], a.n);
+    ++P;
+    if (nfar == 0) break;  // nothing left anywhere
+    if (gtid == 0) {
+      rc->head = rc->tail;  // tickets still waiting when the bucket ended are void
+      ctl->min_bucket = 0xFFFFFFFFu;
+      ctl->buckets += 1;
+      ctl->far_count[fp ^ 1] = 0;
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    // R1: minimum bucket among far entries not yet settled
+    {
+      uint32_t mb = 0xFFFFFFFFu;
+      for (uint64_t i = gtid; i < nfar; i += gthreads) {
+        const uint32_t dd = a.dist[farq[i]];
+        if (dd >= hi) mb = min(mb, dd >> a.shift);
+      }
+      mb = __reduce_min_sync(kFull, mb);
+      if (lane == 0 && mb != 0xFFFFFFFFu) atomicMin(&ctl->min_bucket, mb);
+    }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    const uint32_t nb = ctl->min_bucket;
+    if (nb == 0xFFFFFFFFu) break;  // every far entry was settled
+    // R2: the entries of bucket nb become pending (their regions queued),
+    // later ones stay in the pile
+    {
+      const uint64_t nhi64 = ((uint64_t)nb + 1) << a.shift;
+      const uint32_t nhi = nhi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)nhi64;
+      uint32_t* keepq = a.far[fp ^ 1];
+      for (uint64_t b0 = gtid - lane; b0 < nfar; b0 += gthreads) {
+        const uint64_t i = b0 + lane;
+        bool keep = false;
+        uint32_t u = 0;
+        if (i < nfar) {
+          u = farq[i];
+          const uint32_t dd = a.dist[u];
+          if (dd >= hi && dd < nhi) region_touch(a, ra, u, &ctl->err);
+          else if (dd >= nhi) keep = true;
+          if (!keep) atomicAnd(&a.infar[u >> 5], ~(1u << (u & 31)));
+        }
+        warp_push(keep, u, keepq, &ctl->far_count[fp ^ 1], a.n, &ctl->err);
+      }
+    }
+    bucket = nb;
+    fp ^= 1;
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+  }
+  my_scanned = warp_sum(my_scanned);
+  my_relax = warp_sum(my_relax);
+  if (lane == 0) {
+    if (my_scanned) atomicAdd(&ctl->scanned, my_scanned);
+    if (my_relax) atomicAdd(&ctl->relax, my_relax);
+  }
+  if (tid == 0 && my_rounds) atomicAdd(&ctl->local_rounds, my_rounds);
+  if (gtid == 0) ctl->phases = (uint32_t)min(rc->chunks + 1, 0xFFFFFFFFull);  // region visits
+}
+
 __global__ void sssp_reach_kernel(const uint32_t* __restrict__ dist, const uint64_t* __restrict__ offs,
                                   uint32_t n, unsigned long long* out) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -955,6 +1378,7 @@ static int finish_sssp(gb_graph* g, const SsspArgs& a, unsigned long long* reach
     stats->edges_scanned = hc->scanned;
     stats->relaxations = hc->relax;
     stats->rounds = hc->phases;
+    stats->pull_rounds = (uint32_t)min(hc->local_rounds, 0xFFFFFFFFull);
     stats->buckets = hc->buckets + 1;
     stats->launches = launches;
     stats->kernel_ms = kt.ms();
@@ -970,6 +1394,55 @@ static int finish_sssp(gb_graph* g, const SsspArgs& a, unsigned long long* reach
   return GB_OK;
 }
 
+// The region kernel (every region's arcs fit in shared memory).
+static int run_sssp_region(gb_graph* g, uint32_t src, uint32_t shift, int flush_every, uint32_t nregions,
+                           uint32_t* dist_out, bool out_dev, gb_stats* stats, cudaStream_t s) {
+  const uint32_t n = g->n;
+  const uint32_t words = (n + 31) / 32;
+  // each region is queued at most once at a time
+  const unsigned long long cap = worklists::ring_capacity((uint64_t)nregions + 1024);
+  const size_t need = carve_size<SsspCtl>(1) + 2 * carve_size<uint32_t>(words) + 2 * carve_size<uint32_t>(n) +
+                      (out_dev ? 0 : carve_size<uint32_t>(n)) + carve_size<unsigned long long>(2) +
+                      carve_size<uint32_t>(nregions) + carve_size<char>(worklists::ring_bytes(cap));
+  int st = ws_reserve(g, need, s);
+  if (st != GB_OK) return st;
+  Carver cv(g->ws);
+  SsspArgs a{};
+  RegionArgs ra{};
+  a.ctl = cv.take<SsspCtl>(1);
+  a.infar = cv.take<uint32_t>(words);
+  a.far[0] = cv.take<uint32_t>(n);
+  a.far[1] = cv.take<uint32_t>(n);
+  unsigned long long* reach = cv.take<unsigned long long>(2);
+  a.dist = out_dev ? dist_out : cv.take<uint32_t>(n);
+  ra.pend = cv.take<uint32_t>(words);
+  ra.rq = cv.take<uint32_t>(nregions);
+  ra.nregions = nregions;
+  a.ring = worklists::ring_layout(cv.take<char>(worklists::ring_bytes(cap)), cap);
+  a.offs = g->offs;
+  a.col = g->col;
+  a.w = g->w;
+  a.n = n;
+  a.src = src;
+  a.shift = shift;
+  a.max_phases = 0x7FFFFFFFu;
+  a.local_depth = flush_every;
+  GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), s));
+  GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(worklists::RingCtl), s));
+  sssp_region_init<<<g->sm_count * 4, 256, 0, s>>>(a, ra);
+  GB_CUDA(cudaGetLastError());
+  const void* kfn = reinterpret_cast<const void*>(&sssp_region);
+  const size_t smem = region_smem_bytes();
+  GB_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = coop_grid(g, kfn, kRegionBlock, smem, 1);
+  if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
+  void* args[] = {&a, &ra};
+  KernelTimer kt(stats != nullptr, s);
+  GB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, kRegionBlock, args, smem, s));
+  kt.stop(s);
+  return finish_sssp(g, a, reach, kt, 2, dist_out, out_dev, stats, s);
+}
+
 int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_stats* stats,
              cudaStream_t s) {
   if (!g->w) GB_FAIL(GB_ERR_ARG, "gb_sssp_delta: graph has no uint32 edge weights");
@@ -983,6 +1456,25 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   // light (entries pack the degree in 16 bits and the begin offset in 48)
   const bool async = t.sssp_async > 0 && local_depth > 0 && g->max_degree <= t.heavy_degree &&
                      g->max_degree < 65536 && g->m < (1ull << 48);
+  // regions in shared memory (asked for): every region's arcs must fit
+  bool region = false;
+  const uint32_t nregions = (uint32_t)(((uint64_t)n + kRegion - 1) / kRegion);
+  if (t.sssp_async == 3) {
+    if (!g->region_arcs) {
+      int rst = ws_reserve(g, 256, s);
+      if (rst != GB_OK) return rst;
+      unsigned long long* dmax = static_cast<unsigned long long*>(g->ws);
+      unsigned long long* hmax = static_cast<unsigned long long*>(g->pinned);
+      GB_CUDA(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), s));
+      region_arcs_kernel<<<g->sm_count * 2, 256, 0, s>>>(g->offs, n, nregions, dmax);
+      GB_CUDA(cudaGetLastError());
+      GB_CUDA(cudaMemcpyAsync(hmax, dmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      GB_CUDA(cudaStreamSynchronize(s));
+      g->region_arcs = *hmax + 1;
+    }
+    region = g->region_arcs - 1 <= kRegionArcs;
+  }
+  if (region) return run_sssp_region(g, src, shift, local_depth, nregions, dist_out, out_dev, stats, s);
   FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
   SweepSched sched{};
   if (!async && g->max_degree > t.heavy_degree) {  // heavy rows of a bitmap frontier come from the tile schedule

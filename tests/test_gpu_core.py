@@ -195,8 +195,9 @@ def test_sssp_async_buckets_bit_exact(cuda_device, shift):
                 want = oracle.sssp_dijkstra(g, src)
                 # 1: asynchronous buckets; 2: the same over fixed-width rows
                 # (degree <= 4 or <= 8; the Erdos-Renyi graph's degree is above 8, so it
-                # takes the plain asynchronous kernel)
-                for mode in (1, 2):
+                # takes the plain asynchronous kernel); 3: regions in shared memory
+                # (the Erdos-Renyi graph's regions hold too many arcs: asynchronous kernel)
+                for mode in (1, 2, 3):
                     dg.set_tuning(local_depth=8, sssp_async=mode)
                     got, st = dg.sssp(src, shift, stats=True)
                     assert (got == want).all(), f"async {mode} n={g.n} src={src}"
@@ -227,6 +228,32 @@ def test_sssp_async_small_ring_and_blocks(cuda_device):
             dg.set_tuning(sssp_async=mode)
             got = dg.sssp(0, 13)
             assert got[0] == 0 and (got[1:] == INF).all()
+
+
+@pytest.mark.parametrize("shift", [13, 8, 0])
+def test_sssp_regions_bit_exact(cuda_device, shift):
+    """Regions of 4096 consecutive ids relaxed in shared memory (tuning
+    sssp_async = 3) against Dijkstra: grids of many regions in file order and
+    in locality order (compact regions), a ragged last region, an
+    unreachable part, and a grid whose regions hold too many arcs (8
+    neighbours: the other kernels run)."""
+    from galois_b200._lib import GB_ORDER_LOCALITY
+    cases = [(grid2d(300, 290), (0, 45000, 86999)), (union(grid2d(150, 100), path_graph(5000)), (7, 16000)),
+             (grid2d(64, 64), (0,)), (grid8(120, 90), (0, 5000))]
+    for g, srcs in cases:
+        assign_weights_u32(g, 1, 255, seed=int(g.n) + shift)
+        for order in (0, GB_ORDER_LOCALITY):
+            with DeviceGraph(g, symmetric=True) as dg:
+                if order:
+                    dg.reorder(order)
+                dg.set_tuning(sssp_async=3)
+                for src in srcs:
+                    want = oracle.sssp_dijkstra(g, src)
+                    got, st = dg.sssp(src, shift, stats=True)
+                    assert (got == want).all(), f"regions n={g.n} order={order} src={src}"
+                    assert st["vertices_reached"] == int((want != INF).sum())
+                    # a second call reuses the cached region check and the workspace
+                    assert (dg.sssp(src, shift) == want).all()
 
 
 def test_sssp_local_queues_rmat(cuda_device):
