@@ -934,6 +934,7 @@ constexpr uint32_t kRegion = 4096;       // vertices per region (a multiple of 3
 constexpr uint32_t kRegionArcs = 16384;  // arcs a region may hold in shared memory
 constexpr uint32_t kRegionOut = 2048;    // outbox: relaxations of arcs leaving the region
 constexpr int kRegionBlock = 512;
+constexpr uint32_t kRegionPoll = kRegion / 32;  // threads that poll the pending words during a flush
 
 struct RegionArgs {
   uint32_t* pend;  // bitmap: vertex lowered from outside its region, to be expanded
@@ -946,7 +947,7 @@ constexpr size_t region_smem_bytes() {
          + sizeof(uint32_t) * (kRegion + 4)      // local row offsets
          + 2 * sizeof(uint32_t) * kRegionArcs    // columns, weights
          + 2 * sizeof(uint16_t) * kRegion        // the two round worklists
-         + 2 * sizeof(uint32_t) * (kRegion / 32) // in-worklist bitmap, pending words taken
+         + 3 * sizeof(uint32_t) * (kRegion / 32) // two listed bitmaps, pending words taken
          + sizeof(uint2) * kRegionOut;           // outbox
 }
 
@@ -988,16 +989,19 @@ __global__ void sssp_region_init(SsspArgs a, RegionArgs ra) {
 }
 
 // u (outside the caller's region) was lowered to a distance inside the
-// bucket: mark it pending and queue its region unless it is queued.  The
-// fences order distance -> pending bit -> queued flag against the region's
-// release, which clears the flag and then reads the pending bits.
+// bucket (the atomicMin has returned): announce it with its pending bit and
+// queue its region unless it is queued.  No fence is needed: every step is an
+// atomic whose result is awaited before the next one is issued, and the
+// region's release (atomicExch of its flag, then a read of its bits) is built
+// the same way, so either this call sees the flag cleared or the release sees
+// the bit.  A bit that was set already was announced by its setter, which
+// took care of the queue, and the region reads the distance after taking the
+// bit.
 __device__ __forceinline__ void region_touch(const SsspArgs& a, const RegionArgs& ra, uint32_t u, int* err) {
-  __threadfence();
-  atomicOr(&ra.pend[u >> 5], 1u << (u & 31));
-  __threadfence();
+  const uint32_t bit = 1u << (u & 31);
+  if (atomicOr(&ra.pend[u >> 5], bit) & bit) return;
   const uint32_t rg = u / kRegion;
-  if (*reinterpret_cast<volatile uint32_t*>(&ra.rq[rg]) == 0u && atomicCAS(&ra.rq[rg], 0u, 1u) == 0u)
-    worklists::publish_one(a.ring, make_uint4(rg, 0u, 0u, 0u), err);
+  if (atomicOr(&ra.rq[rg], 1u) == 0u) worklists::publish_one(a.ring, make_uint4(rg, 0u, 0u, 0u), err);
 }
 
 // File u (lowered to a distance beyond the bucket) in the far pile once.
@@ -1071,9 +1075,9 @@ __global__ void __launch_bounds__(kRegionBlock, 1) sssp_region(SsspArgs a, Regio
   uint32_t* s_col = s_loff + kRegion + 4;
   uint32_t* s_w = s_col + kRegionArcs;
   uint2* s_out = reinterpret_cast<uint2*>(s_w + kRegionArcs);
-  uint32_t* s_inq = reinterpret_cast<uint32_t*>(s_out + kRegionOut);
-  uint32_t* s_pw = s_inq + kRegion / 32;
-  uint16_t* s_wl = reinterpret_cast<uint16_t*>(s_pw + kRegion / 32);  // [2][kRegion]
+  uint32_t* s_bm = reinterpret_cast<uint32_t*>(s_out + kRegionOut);  // [2][kRegion / 32] listed bitmaps
+  uint32_t* s_pw = s_bm + 2 * (kRegion / 32);                          // pending words taken
+  uint16_t* s_wl = reinterpret_cast<uint16_t*>(s_pw + kRegion / 32);   // [2][kRegion] round lists
   __shared__ uint32_t s_region, s_go, s_n[3], s_nout;
   const uint32_t flush_every = a.local_depth > 0 ? (uint32_t)a.local_depth : 8u;
   SsspCtl* ctl = a.ctl;
@@ -1120,12 +1124,13 @@ __global__ void __launch_bounds__(kRegionBlock, 1) sssp_region(SsspArgs a, Regio
       const uint64_t o0 = ldg(a.offs + base);
       const uint32_t na = (uint32_t)(ldg(a.offs + base + nv) - o0);
       if (tid == 0) s_n[0] = s_n[1] = s_n[2] = s_nout = 0;
+      for (uint32_t j = tid; j < kRegion / 32; j += kRegionBlock) s_bm[kRegion / 32 + j] = 0u;
       __syncthreads();
       // the pending vertices start the worklist; they are taken before the
       // distances are read, so a lowering after this point sets its bit again
       for (uint32_t j = tid; j < kRegion / 32; j += kRegionBlock) {
         uint32_t bits = j < nw ? atomicExch(&ra.pend[(base >> 5) + j], 0u) : 0u;
-        s_inq[j] = bits;
+        s_bm[j] = bits;
         if (bits) {
           const uint32_t pos = atomicAdd(&s_n[0], (uint32_t)__popc(bits));
           for (uint32_t k = 0; bits; ++k, bits &= bits - 1) s_wl[pos + k] = (uint16_t)(j * 32 + __ffs(bits) - 1);
@@ -1135,36 +1140,34 @@ __global__ void __launch_bounds__(kRegionBlock, 1) sssp_region(SsspArgs a, Regio
       __syncthreads();
       region_load(a, base, nv, o0, na, s_dist, s_loff, s_col, s_w);
       __syncthreads();
-      // local rounds: every listed vertex's arcs, in shared memory inside the
-      // region; an arc that leaves the region goes to the outbox, which is
-      // flushed to the global distances every `flush_every` rounds (and when
-      // the round list runs dry or the outbox fills), so no round waits on a
-      // global atomic; each flush also takes in this region's vertices
-      // lowered from outside meanwhile
       // Round k relaxes list k & 1 (count s_n[k % 3]) into list (k + 1) & 1
-      // (count s_n[(k + 1) % 3]) and zeroes s_n[(k + 2) % 3], so one CTA
-      // barrier per round suffices.  Four lanes share a list entry, one arc
-      // each; appends are aggregated per warp.
+      // (count s_n[(k + 1) % 3], listed bitmap (k + 1) & 1) and clears
+      // bitmap k & 1 and s_n[(k + 2) % 3], which no thread uses in round k,
+      // so one CTA barrier per round suffices.  A vertex lowered while its
+      // entry is being expanded is listed again for the next round, so the
+      // expansion may read its distance at any time.  Four lanes share an
+      // entry, one arc each; appends are per warp.  An arc that leaves the
+      // region goes to the outbox, flushed every `flush_every` rounds and
+      // when the list runs dry: the outbox into the global distances
+      // (queueing the targets' regions or filing them far) while threads
+      // 0-127 take this region's pending bits, whose vertices then join the
+      // next round.
       const uint32_t lanemask_lt = (1u << lane) - 1u;
       uint32_t k = 0, since = 0;
       for (;; ++k) {
         const uint32_t cnt = s_n[k % 3];
         const uint16_t* wl = s_wl + (k & 1) * kRegion;
         uint16_t* wl_next = s_wl + ((k + 1) & 1) * kRegion;
+        uint32_t* bm_next = s_bm + ((k + 1) & 1) * (kRegion / 32);
         uint32_t* n_next = &s_n[(k + 1) % 3];
         if (tid == 0) s_n[(k + 2) % 3] = 0;
+        if (tid < kRegion / 32) s_bm[(k & 1) * (kRegion / 32) + tid] = 0u;
         for (uint32_t i0 = (tid >> 5) * 8; i0 < cnt; i0 += kRegionBlock / 4) {  // warp-uniform
           const uint32_t i = i0 + (lane >> 2), sub = lane & 3u;
           const bool has = i < cnt;
           const uint32_t v = has ? (uint32_t)wl[i] : 0u;
-          uint32_t d = hi;
-          if (has && sub == 0) {
-            atomicAnd(&s_inq[v >> 5], ~(1u << (v & 31)));
-            __threadfence_block();
-            d = *reinterpret_cast<volatile uint32_t*>(&s_dist[v]);
-          }
-          d = __shfl_sync(kFull, d, lane & ~3u);
-          const bool live = has && d < hi;
+          const uint32_t d = has ? *reinterpret_cast<volatile uint32_t*>(&s_dist[v]) : hi;
+          const bool live = d < hi;
           uint32_t j = live ? s_loff[v] + sub : 0u;
           const uint32_t e1 = live ? s_loff[v + 1] : 0u;
           while (__any_sync(kFull, j < e1)) {
@@ -1180,7 +1183,7 @@ __global__ void __launch_bounds__(kRegionBlock, 1) sssp_region(SsspArgs a, Regio
                 if (nd < *reinterpret_cast<volatile uint32_t*>(&s_dist[lu]) && nd < atomicMin(&s_dist[lu], nd)) {
                   ++my_relax;
                   const uint32_t bit = 1u << (lu & 31);
-                  to_next = nd < hi && !(atomicOr(&s_inq[lu >> 5], bit) & bit);
+                  to_next = nd < hi && !(atomicOr(&bm_next[lu >> 5], bit) & bit);
                 }
               } else {
                 to_out = true;
@@ -1204,7 +1207,7 @@ __global__ void __launch_bounds__(kRegionBlock, 1) sssp_region(SsspArgs a, Regio
               if (to_out) {
                 if (pos < kRegionOut) {
                   s_out[pos] = make_uint2(u, nd);
-                } else if (nd < __ldcg(a.dist + u) && nd < atomicMin(&a.dist[u], nd)) {  // outbox full
+                } else if (nd < atomicMin(&a.dist[u], nd)) {  // outbox full
                   ++my_relax;
                   if (nd < hi) region_touch(a, ra, u, &ctl->err);
                   else far_file(a, farq, far_count, u, &ctl->err);
@@ -1214,24 +1217,27 @@ __global__ void __launch_bounds__(kRegionBlock, 1) sssp_region(SsspArgs a, Regio
           }
         }
         __syncthreads();
-        // uniform: s_n[(k + 1) % 3] and s_nout change only after the next
-        // barrier (round k + 1 appends to s_n[(k + 2) % 3])
+        // uniform: s_n[(k + 1) % 3] changes only after the next barrier
         if (*n_next != 0 && ++since < flush_every) continue;
         since = 0;
-        const uint32_t no = min(s_nout, kRegionOut);
-        for (uint32_t i = tid; i < no; i += kRegionBlock) {
-          const uint2 o = s_out[i];
-          if (o.y < atomicMin(&a.dist[o.x], o.y)) {
-            ++my_relax;
-            if (o.y < hi) region_touch(a, ra, o.x, &ctl->err);
-            else far_file(a, farq, far_count, o.x, &ctl->err);
+        if (tid < kRegionPoll) {
+          // take the pending bits before reading the distances they announce
+          uint32_t bits = 0;
+          if (tid < nw) {
+            bits = *reinterpret_cast<volatile uint32_t*>(&ra.pend[(base >> 5) + tid]);
+            if (bits) bits = atomicExch(&ra.pend[(base >> 5) + tid], 0u);
           }
-        }
-        // take the pending bits before reading the distances they announce
-        for (uint32_t j = tid; j < nw; j += kRegionBlock) {
-          uint32_t bits = *reinterpret_cast<volatile uint32_t*>(&ra.pend[(base >> 5) + j]);
-          if (bits) bits = atomicExch(&ra.pend[(base >> 5) + j], 0u);
-          s_pw[j] = bits;
+          s_pw[tid] = bits;
+        } else {
+          const uint32_t no = min(s_nout, kRegionOut);
+          for (uint32_t i = tid - kRegionPoll; i < no; i += kRegionBlock - kRegionPoll) {
+            const uint2 o = s_out[i];
+            if (o.y < atomicMin(&a.dist[o.x], o.y)) {
+              ++my_relax;
+              if (o.y < hi) region_touch(a, ra, o.x, &ctl->err);
+              else far_file(a, farq, far_count, o.x, &ctl->err);
+            }
+          }
         }
         __threadfence();
         __syncthreads();
@@ -1246,7 +1252,7 @@ __global__ void __launch_bounds__(kRegionBlock, 1) sssp_region(SsspArgs a, Regio
           if (gd <= s_dist[i]) {
             s_dist[i] = gd;  // no relaxation runs during the flush
             const uint32_t bit = 1u << (i & 31);
-            if (gd < hi && !(atomicOr(&s_inq[i >> 5], bit) & bit)) wl_next[atomicAdd(n_next, 1u)] = (uint16_t)i;
+            if (gd < hi && !(atomicOr(&bm_next[i >> 5], bit) & bit)) wl_next[atomicAdd(n_next, 1u)] = (uint16_t)i;
           }
         }
         __syncthreads();
@@ -1264,11 +1270,9 @@ __global__ void __launch_bounds__(kRegionBlock, 1) sssp_region(SsspArgs a, Regio
       if (tid == 0) {
         __threadfence();
         atomicExch(&ra.rq[r], 0u);
-        __threadfence();
       }
       __syncthreads();
       if (tid < 32) {
-        __threadfence();
         bool any = false;
         for (uint32_t j = tid; j < nw; j += 32)
           any |= *reinterpret_cast<volatile uint32_t*>(&ra.pend[(base >> 5) + j]) != 0u;
