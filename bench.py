@@ -47,9 +47,11 @@ def parse_args():
     ap.add_argument("--size", choices=["small", "medium", "full", "s24"], default="full",
                     help="graph sizes: full = the benchmark configuration; s24 = RMAT scale 24 for every "
                          "app; medium/small for profiling")
-    ap.add_argument("--order", type=int, choices=[0, 1, 2], default=1,
-                    help="vertex order of the resident graph: 0 file order, 1 degree-ordered with sorted "
-                         "rows (gb_graph_reorder, done once before timing), 2 degree-ordered unsorted rows")
+    ap.add_argument("--order", type=int, choices=[0, 1, 2, 3, 4], default=4,
+                    help="vertex order of the resident graphs (gb_graph_reorder, done once before timing): "
+                         "0 file order, 1 degree-ordered with sorted rows, 2 degree-ordered unsorted rows, "
+                         "3 locality (Morton order of landmark BFS distances), 4 auto (3 when no vertex has "
+                         "more than 16 arcs, else 1)")
     ap.add_argument("--small", action="store_true", help="same as --size small")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -599,7 +601,9 @@ class PrResidualJob(PrJob):
 
 JOBS = {"sssp": SsspJob, "bfs": BfsJob, "bfs-parent": BfsParentJob, "cc": CcJob, "pr": PrJob, "pr-residual": PrResidualJob}
 ORDER_NAMES = {0: "file order", 1: "degree-ordered (gb_graph_reorder, sorted rows)",
-               2: "degree-ordered (gb_graph_reorder, unsorted rows)"}
+               2: "degree-ordered (gb_graph_reorder, unsorted rows)",
+               3: "locality (gb_graph_reorder: Morton order of landmark BFS distances, sorted rows)",
+               4: "auto (gb_graph_reorder: locality for degree <= 16, else degree-ordered)"}
 BATCHED = ("bc", "multigraph", "ppr")
 
 
@@ -883,7 +887,7 @@ def measure_resident(job: Job, dev: int, dist: Dist, steps: int, warmup: int, or
     clk = clocks.stop()
     t_ms = dist.max(e0.elapsed_time(e1))
     return {"dgs": dgs, "outs": outs, "stats": stats, "kms": kms, "t_ms": t_ms, "clocks": clk,
-            "reorder_ms": reorder_ms,
+            "reorder_ms": reorder_ms, "orders": [dg.order for dg in dgs],
             "units_step": sum(job.units(st, gi) for gi, st in enumerate(stats)),
             "bytes_step": sum(job.algo_bytes(st, gi) for gi, st in enumerate(stats)),
             "work_step": sum(job.work_bytes(st, gi) for gi, st in enumerate(stats))}
@@ -897,11 +901,17 @@ def roofline_of(job: Job, r: dict, order: int, traffic) -> dict:
     the model, label-correcting SSSP more); both are kept beside it."""
     peak, peak_src = measured_peak_hbm()
     sec = sum(r["kms"]) / 1e3
+    kernel = job.kernel
+    if type(job) is PrJob and 1 in r["orders"]:
+        kernel = "pr_pull_flat"  # a degree-ordered PageRank runs the flat pull kernels
+    elif type(job) is SsspJob:
+        # the region kernel reports its shared-memory rounds in pull_rounds
+        kernel = " + ".join(f"{'sssp_region' if st.get('pull_rounds') else 'sssp_persistent'} ({g['name']})"
+                            for g, st in zip(job.graphs, r["stats"]))
     need = min(r["bytes_step"], r["work_step"])
     return {"bound": "hbm", "achieved": need / sec / 1e9, "peak": peak, "unit": "GB/s",
             "frac": need / sec / 1e9 / peak, "peak_source": peak_src,
-            # a degree-ordered PageRank runs the flat pull kernels
-            "kernel": "pr_pull_flat" if (type(job) is PrJob and order) else job.kernel,
+            "kernel": kernel,
             "bytes_counted_per_step": need,
             "algorithmic_bytes_per_step": r["bytes_step"], "kernel_ms_per_step": sum(r["kms"]),
             "model_frac": r["bytes_step"] / sec / 1e9 / peak,
@@ -1094,7 +1104,9 @@ def main() -> None:
     line = {"metric": job.metric, "value": value, "unit": job.unit, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": job.dtype, "data": "synthetic (seeded generators)",
-            "config": {**job.config(), "vertex_order": ORDER_NAMES[args.order]}, "roofline": roofline,
+            "config": {**job.config(), "vertex_order": ORDER_NAMES[args.order],
+                       "orders": {job.graphs[gi]["name"]: ORDER_NAMES[o] for gi, o in enumerate(r["orders"])}},
+            "roofline": roofline,
             "clocks": r["clocks"],
             "gpu_launches": sum(int(st["launches"]) for st in stats) * args.steps,
             "reorder_ms": r["reorder_ms"],

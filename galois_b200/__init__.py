@@ -12,14 +12,15 @@ All compute goes through libgb.so (include/gb.h); importing this package
 without the built library raises ImportError.
 """
 from . import _lib  # noqa: F401  (loads libgb.so or fails loudly)
-from ._lib import (GB_CC_AFFOREST, GB_CC_LABELPROP, GB_CC_UNIONFIND, GB_DIST_INFINITY, GB_ORDER_DEGREE,
-                   GB_ORDER_DEGREE_UNSORTED, GB_ORDER_NONE, GbError)
+from ._lib import (GB_CC_AFFOREST, GB_CC_LABELPROP, GB_CC_UNIONFIND, GB_DIST_INFINITY, GB_ORDER_AUTO,
+                   GB_ORDER_DEGREE, GB_ORDER_DEGREE_UNSORTED, GB_ORDER_LOCALITY, GB_ORDER_NONE, GbError)
 from .device import DeviceGraph
 from .graph import (HostCSR, assign_weights_f32, assign_weights_reference, assign_weights_u32, csr_to_edgelist,
                     edgelist_to_csr, erdos_renyi, grid2d, read_gr, rmat, transpose, write_gr)
 
 __all__ = [
     "DeviceGraph", "HostCSR", "GbError", "GB_DIST_INFINITY", "GB_CC_LABELPROP", "GB_CC_UNIONFIND",
-    "GB_CC_AFFOREST", "GB_ORDER_NONE", "GB_ORDER_DEGREE", "GB_ORDER_DEGREE_UNSORTED", "read_gr", "write_gr",
+    "GB_CC_AFFOREST", "GB_ORDER_NONE", "GB_ORDER_DEGREE", "GB_ORDER_DEGREE_UNSORTED",
+    "GB_ORDER_LOCALITY", "GB_ORDER_AUTO", "read_gr", "write_gr",
     "rmat", "grid2d", "erdos_renyi", "assign_weights_u32", "assign_weights_reference", "assign_weights_f32", "transpose", "edgelist_to_csr", "csr_to_edgelist",
 ]

@@ -30,6 +30,7 @@ GB_ORDER_NONE = 0
 GB_ORDER_DEGREE = 1
 GB_ORDER_DEGREE_UNSORTED = 2
 GB_ORDER_LOCALITY = 3
+GB_ORDER_AUTO = 4
 GB_PR_PUSH_ASYNC = 0
 GB_PR_PUSH_SYNC = 1
 
@@ -124,6 +125,7 @@ SIGNATURES: dict[str, tuple] = {
     "gb_graph_reorder": (C.c_int, [_gp, C.c_int, _vp]),
     "gb_pool_trim": (C.c_int, []),
     "gb_graph_permutation": (C.c_int, [_gp, C.POINTER(_vp), C.POINTER(_vp)]),
+    "gb_graph_order": (C.c_int, [_gp, C.POINTER(C.c_int)]),
     "gb_graph_set_tuning": (C.c_int, [_gp, C.POINTER(Tuning)]),
     "gb_graph_get_tuning": (C.c_int, [_gp, C.POINTER(Tuning)]),
     "gb_bfs": (C.c_int, [_gp, C.c_uint32, _vp, C.POINTER(Stats), _vp]),

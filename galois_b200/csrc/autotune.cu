@@ -124,6 +124,10 @@ extern "C" int gb_autotune(gb_graph* g, const char* kernel, uint32_t src, const 
             cands.push_back(t);
             t.sssp_async = 2;
             cands.push_back(t);
+            if (g->order == GB_ORDER_LOCALITY) {  // 0 took the regions: also without them
+              t.sssp_async = -1;
+              cands.push_back(t);
+            }
           }
         }
       } else if (k == "bfs") {

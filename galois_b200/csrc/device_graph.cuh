@@ -46,8 +46,10 @@ struct gb_graph {
   // vertex, columns then uint32 weights, empty slots 0xFFFFFFFF), for SSSP
   uint32_t* ell = nullptr;
   uint32_t ell_d = 0;
-  // largest arc count of a 4096-vertex region + 1 (0: not computed), for SSSP
+  // largest arc count of a 4096-vertex region + 1 (0: not computed) and the
+  // fraction of arcs inside their region, for SSSP
   uint64_t region_arcs = 0;
+  double region_local = 0.0;
   uint32_t max_degree = 0;
   // all-vertex sweep schedule (sweep.cuh), cached per (heavy, tile)
   uint2* sweep_tiles = nullptr;

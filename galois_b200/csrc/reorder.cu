@@ -280,6 +280,7 @@ int reorder_graph(gb_graph* g, int order, cudaStream_t s) {
     if (g->perm) GB_FAIL(GB_ERR_UNSUPPORTED, "gb_graph_reorder: a relabelled graph cannot be restored");
     return GB_OK;
   }
+  if (order == GB_ORDER_AUTO) order = g->max_degree <= 16 ? GB_ORDER_LOCALITY : GB_ORDER_DEGREE;
   if (order != GB_ORDER_DEGREE && order != GB_ORDER_DEGREE_UNSORTED && order != GB_ORDER_LOCALITY)
     GB_FAIL(GB_ERR_ARG, "gb_graph_reorder: unknown order %d", order);
   if (g->perm) {
@@ -494,6 +495,13 @@ extern "C" int gb_graph_reorder(gb_graph* g, int order, void* stream) {
   if (!g) GB_FAIL(GB_ERR_ARG, "gb_graph_reorder: null graph");
   GB_CUDA(cudaSetDevice(g->device));
   return reorder_graph(g, order, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int gb_graph_order(const gb_graph* g, int* order) {
+  clear_error();
+  if (!g || !order) GB_FAIL(GB_ERR_ARG, "gb_graph_order: null argument");
+  *order = g->perm ? g->order : GB_ORDER_NONE;
+  return GB_OK;
 }
 
 extern "C" int gb_graph_permutation(const gb_graph* g, const uint32_t** new_to_old, const uint32_t** old_to_new) {

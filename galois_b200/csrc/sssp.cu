@@ -951,17 +951,30 @@ constexpr size_t region_smem_bytes() {
          + sizeof(uint2) * kRegionOut;           // outbox
 }
 
-// Largest arc count of any region (host check that regions fit).
-__global__ void region_arcs_kernel(const uint64_t* __restrict__ offs, uint32_t n, uint32_t nregions,
-                                   unsigned long long* max_arcs) {
+// Largest arc count of any region (out[0], the host check that regions fit)
+// and the number of arcs whose two ends share a region (out[1]).
+__global__ void region_arcs_kernel(const uint64_t* __restrict__ offs, const uint32_t* __restrict__ col, uint32_t n,
+                                   uint32_t nregions, unsigned long long* out) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  unsigned long long mine = 0;
-  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < nregions; r += stride) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  unsigned long long mine = 0, local = 0;
+  for (uint64_t r = tid; r < nregions; r += stride) {
     const uint64_t b = r * kRegion, e = b + kRegion < (uint64_t)n ? b + kRegion : (uint64_t)n;
     mine = max(mine, (unsigned long long)(offs[e] - offs[b]));
   }
-  for (int o = 16; o > 0; o >>= 1) mine = max(mine, __shfl_xor_sync(kFull, mine, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(max_arcs, mine);
+  // arcs by row: a thread per vertex
+  for (uint64_t v = tid; v < n; v += stride) {
+    const uint64_t r = v / kRegion;
+    for (uint64_t j = offs[v]; j < offs[v + 1]; ++j) local += (uint64_t)col[j] / kRegion == r;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mine = max(mine, __shfl_xor_sync(kFull, mine, o));
+    local += __shfl_xor_sync(kFull, local, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, mine);
+    atomicAdd(out + 1, local);
+  }
 }
 
 __global__ void sssp_region_init(SsspArgs a, RegionArgs ra) {
@@ -1460,23 +1473,28 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
   // light (entries pack the degree in 16 bits and the begin offset in 48)
   const bool async = t.sssp_async > 0 && local_depth > 0 && g->max_degree <= t.heavy_degree &&
                      g->max_degree < 65536 && g->m < (1ull << 48);
-  // regions in shared memory (asked for): every region's arcs must fit
+  // regions in shared memory: asked for (sssp_async 3: whenever every
+  // region's arcs fit), or by default on a graph numbered by locality whose
+  // regions fit and keep at least 90 % of the arcs inside (measured on the
+  // 4096^2 grid: 29.3 ms against 38.5 ms for the phase-synchronous kernel)
   bool region = false;
   const uint32_t nregions = (uint32_t)(((uint64_t)n + kRegion - 1) / kRegion);
-  if (t.sssp_async == 3) {
-    if (!g->region_arcs) {
+  if (t.sssp_async == 3 || (t.sssp_async == 0 && g->order == GB_ORDER_LOCALITY)) {
+    if (!g->region_arcs) {  // once per graph (and after a relabelling)
       int rst = ws_reserve(g, 256, s);
       if (rst != GB_OK) return rst;
-      unsigned long long* dmax = static_cast<unsigned long long*>(g->ws);
-      unsigned long long* hmax = static_cast<unsigned long long*>(g->pinned);
-      GB_CUDA(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), s));
-      region_arcs_kernel<<<g->sm_count * 2, 256, 0, s>>>(g->offs, n, nregions, dmax);
+      unsigned long long* dout = static_cast<unsigned long long*>(g->ws);
+      unsigned long long* hout = static_cast<unsigned long long*>(g->pinned);
+      GB_CUDA(cudaMemsetAsync(dout, 0, 2 * sizeof(unsigned long long), s));
+      region_arcs_kernel<<<g->sm_count * 8, 256, 0, s>>>(g->offs, g->col, n, nregions, dout);
       GB_CUDA(cudaGetLastError());
-      GB_CUDA(cudaMemcpyAsync(hmax, dmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      GB_CUDA(cudaMemcpyAsync(hout, dout, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
       GB_CUDA(cudaStreamSynchronize(s));
-      g->region_arcs = *hmax + 1;
+      g->region_arcs = hout[0] + 1;
+      g->region_local = g->m ? (double)hout[1] / (double)g->m : 1.0;
     }
-    region = g->region_arcs - 1 <= kRegionArcs;
+    const bool fits = g->region_arcs - 1 <= kRegionArcs;
+    region = t.sssp_async == 3 ? fits : fits && g->region_local >= 0.9;
   }
   if (region) return run_sssp_region(g, src, shift, local_depth, nregions, dist_out, out_dev, stats, s);
   FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);

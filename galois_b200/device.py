@@ -69,6 +69,14 @@ class DeviceGraph:
     def reorder(self, order: int = _lib.GB_ORDER_DEGREE) -> None:
         check(lib.gb_graph_reorder(self.handle, int(order), None), "gb_graph_reorder")
 
+    @property
+    def order(self) -> int:
+        """The order the graph was relabelled with (GB_ORDER_NONE if never;
+        GB_ORDER_AUTO reports the order it chose)."""
+        o = C.c_int()
+        check(lib.gb_graph_order(self.handle, C.byref(o)), "gb_graph_order")
+        return o.value
+
     def permutation(self) -> dict:
         """Device pointers of the relabelling (None when in file order)."""
         p = [C.c_void_p() for _ in range(2)]

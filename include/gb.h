@@ -206,7 +206,13 @@ int gb_graph_assign_weights_f32(gb_graph* g, uint64_t seed, void* stream);
  * farthest from vertex 0, the one farthest from it, and the one farthest
  * from both), so consecutive ids form compact 2-D patches; rows are sorted. */
 #define GB_ORDER_LOCALITY 3
+/* GB_ORDER_AUTO: GB_ORDER_LOCALITY when no vertex has more than 16 stored
+ * arcs, else GB_ORDER_DEGREE. */
+#define GB_ORDER_AUTO 4
 int gb_graph_reorder(gb_graph* g, int order, void* stream);
+/* The order a graph was relabelled with (GB_ORDER_NONE if it never was;
+ * GB_ORDER_AUTO reports the order it chose). */
+int gb_graph_order(const gb_graph* g, int* order);
 /* Device permutation of a reordered graph: new_to_old[internal id] =
  * original id, old_to_new the inverse; both NULL if not reordered. */
 int gb_graph_permutation(const gb_graph* g, const uint32_t** new_to_old,
@@ -252,8 +258,11 @@ typedef struct gb_tuning {
                             GB_ORDER_LOCALITY; otherwise as 1); stats:
                             rounds = region visits, pull_rounds =
                             shared-memory rounds;
-                            <= 0 = library default (a grid barrier after
-                            every phase) */
+                            0 = library default: regions on a
+                            GB_ORDER_LOCALITY graph whose regions fit and
+                            keep >= 90 % of the arcs inside, else a grid
+                            barrier after every phase; < 0 = a grid
+                            barrier after every phase */
 } gb_tuning;
 int gb_graph_set_tuning(gb_graph* g, const gb_tuning* t);
 int gb_graph_get_tuning(const gb_graph* g, gb_tuning* t);

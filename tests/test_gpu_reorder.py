@@ -205,7 +205,7 @@ def test_locality_order_all_algorithms(cuda_device):
             for src in srcs:
                 assert (dg.bfs(src) == oracle.bfs_serial(h, src)).all()
                 want = oracle.sssp_dijkstra(h, src)
-                for mode in (0, 1):
+                for mode in (0, 1, -1):
                     dg.set_tuning(sssp_async=mode)
                     assert (dg.sssp(src, 13) == want).all(), (h.n, src, mode)
             assert (dg.cc(GB_CC_LABELPROP) == oracle.cc_union_find(h)).all()
@@ -218,3 +218,30 @@ def test_locality_order_all_algorithms(cuda_device):
     rows, cols = old // 70, old % 70
     hop = np.abs(np.diff(rows)) + np.abs(np.diff(cols))
     assert np.median(hop) <= 2
+
+
+def test_auto_order_and_default_region_kernel(cuda_device):
+    """GB_ORDER_AUTO numbers a bounded-degree grid by locality and an RMAT
+    graph by degree; on the locality-ordered grid the default SSSP takes the
+    shared-memory region kernel (its statistics report shared-memory rounds),
+    sssp_async = -1 the phase-synchronous one; both exact, several sources,
+    a bucket width of 1 and of 2^13."""
+    from galois_b200 import GB_ORDER_AUTO
+    g = grid2d(180, 200)
+    assign_weights_u32(g, 1, 255, seed=5)
+    r, _ = rmat(12, 8, seed=3)
+    with DeviceGraph(r, symmetric=True, reorder=GB_ORDER_AUTO) as dg:
+        assert dg.order == GB_ORDER_DEGREE
+    with DeviceGraph(g, symmetric=True) as dg:
+        assert dg.order == GB_ORDER_NONE
+        dg.reorder(GB_ORDER_AUTO)
+        assert dg.order == GB_ORDER_LOCALITY
+        for src in (0, 17999, 35999):
+            for shift in (13, 0):
+                want = oracle.sssp_dijkstra(g, src)
+                got, st = dg.sssp(src, shift, stats=True)
+                assert (got == want).all() and st["pull_rounds"] > 0, (src, shift)
+                dg.set_tuning(sssp_async=-1)
+                got, st = dg.sssp(src, shift, stats=True)
+                assert (got == want).all() and st["pull_rounds"] == 0, (src, shift)
+                dg.set_tuning(sssp_async=0)
