@@ -339,7 +339,7 @@ class SsspJob(Job):
         from galois_b200 import assign_weights_u32, grid2d, rmat
 
         scale, side = pick(size, (16, 512), (20, 2048), (22, 4096), (24, 4096))
-        self.workload = self.workload.replace("RMAT-22", f"RMAT-{scale}")
+        self.workload = self.workload.replace("RMAT-22", f"RMAT-{scale}").replace("4096x4096", f"{side}x{side}")
         g, perm = rmat(scale, 16, seed=22, symmetrize=False)
         assign_weights_u32(g, 1, 255, seed=22)
         self.graphs.append({"name": f"rmat{scale}-directed", "host": g, "symmetric": False, "src": int(perm[0])})

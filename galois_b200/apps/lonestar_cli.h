@@ -141,7 +141,8 @@ inline void load(const Flags& f, int edge_bytes, Loaded& L) {
   check(gb_graph_upload(L.h.end_offs, L.h.col, L.h.w_u32, L.h.w_f32, L.h.n, L.h.m,
                         f.flag("symmetricGraph") ? 1 : 0, (int)f.u64("device", 0), &L.g),
         "gb_graph_upload");
-  // -reorder=1|2: relabel the device mirror by degree (results stay in file ids)
+  // -reorder=1|2|3|4: relabel the device mirror (degree, degree without the row
+  // sort, locality, auto); results stay in file ids
   const int order = (int)f.u64("reorder", 0);
   if (order) check(gb_graph_reorder(L.g, order, nullptr), "gb_graph_reorder");
 }
