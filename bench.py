@@ -903,7 +903,7 @@ def roofline_of(job: Job, r: dict, order: int, traffic) -> dict:
     sec = sum(r["kms"]) / 1e3
     kernel = job.kernel
     if type(job) is PrJob and 1 in r["orders"]:
-        kernel = "pr_pull_flat"  # a degree-ordered PageRank runs the flat pull kernels
+        kernel = "pr_pull_binned"  # a degree-ordered PageRank runs the binned pull kernel
     elif type(job) is SsspJob:
         # the region kernel reports its shared-memory rounds in pull_rounds
         kernel = " + ".join(f"{'sssp_region' if st.get('pull_rounds') else 'sssp_persistent'} ({g['name']})"

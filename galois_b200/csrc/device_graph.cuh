@@ -42,6 +42,9 @@ struct gb_graph {
   uint32_t lr_row0 = 0, lr_heavy = 0;
   uint64_t lr_arc0 = 0, lr_arc1 = 0;
   float* colsum = nullptr;               // PPR column sums of wf by source
+  // PageRank pull on degree-ordered graphs: the binned layout of the arcs
+  // (opaque, built and freed by pagerank.cu)
+  struct PrBins* prb = nullptr;
   // bounded-degree graphs: the arcs as fixed-width rows (ell_d slots per
   // vertex, columns then uint32 weights, empty slots 0xFFFFFFFF), for SSSP
   uint32_t* ell = nullptr;
@@ -148,6 +151,8 @@ int copy_in(void* dst_dev, const void* src, size_t bytes, cudaStream_t stream);
 int ensure_transpose(gb_graph* g, cudaStream_t stream);
 // Frees every cached array derived from the stored arcs (reorder.cu).
 void drop_derived(gb_graph* g);
+// Frees the PageRank binned layout (pagerank.cu).
+void free_pr_bins(gb_graph* g);
 
 // Relabelled graphs (reorder.cu).  result_buf returns the k-th n-word
 // staging buffer (k < 3).  finish_* map a result computed in internal ids

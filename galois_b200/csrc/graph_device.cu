@@ -404,6 +404,7 @@ int gb_graph_free(gb_graph* g) {
   cudaFree(g->t_emap);
   cudaFree(g->outdeg_of_stored);
   cudaFree(g->lr_rowid);
+  gb::free_pr_bins(g);
   cudaFree(g->colsum);
   cudaFree(g->ell);
   if (g->ppr_free) g->ppr_free(g);

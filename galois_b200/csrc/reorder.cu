@@ -209,6 +209,7 @@ void drop_derived(gb_graph* g) {
   cudaFree(g->outdeg_of_stored);
   cudaFree(g->lr_rowid);
   g->lr_rowid = nullptr;
+  free_pr_bins(g);
   cudaFree(g->colsum);
   g->outdeg_of_stored = nullptr;
   g->colsum = nullptr;
