@@ -517,14 +517,64 @@ __device__ __forceinline__ void bin_add(float* s_sum, const uint4& dd, const flo
   for (int k = 1; k < 8; ++k) {
     const uint32_t d = bin_dst(dd, k);
     if (d != cur) {
-      if (cur != kBinPad) atomicAdd(&s_sum[cur], run);
+      if (cur != kBinPad && run != 0.f) atomicAdd(&s_sum[cur], run);
       cur = d;
       run = x[k];
     } else {
       run += x[k];
     }
   }
-  if (cur != kBinPad) atomicAdd(&s_sum[cur], run);
+  if (cur != kBinPad && run != 0.f) atomicAdd(&s_sum[cur], run);
+}
+
+// The gather phase of a binned iteration: the CTA takes tasks until none is
+// left and leaves in every destination's sum slot of acc_cur the sum of
+// c_in over its in-arcs.  All threads of the CTA call.
+template <int BLOCK>
+__device__ __forceinline__ void bin_gather(const PrArgs& a, const float* c_in, float* acc_cur, uint32_t it, float* s_sum,
+                                           uint32_t* s_task) {
+  const uint32_t tid = threadIdx.x, lane = lane_id(), wib = tid >> 5;
+  constexpr uint32_t kW = BLOCK / 32;
+    for (;;) {
+      if (tid == 0) *s_task = atomicAdd(&a.ctl->task_next[it & 1], 1u);
+      __syncthreads();
+      const uint32_t t = *s_task;
+      if (t >= a.b_ntasks) break;  // uniform
+      const uint4 tk = ldg(a.b_tasks + t);
+      const uint32_t v0 = tk.x, nv = tk.y & 0x7FFFFFFFu;
+      const bool multi = (tk.y >> 31) != 0u;
+      for (uint32_t d = tid; d < nv; d += BLOCK) s_sum[d] = 0.f;
+      __syncthreads();
+      // a lane takes 8 consecutive arcs of a chunk (sorted by destination
+      // inside the chunk, so equal destinations are summed in registers
+      // before one shared-memory atomic); the next chunk's words load while
+      // this chunk's contributions are read and added (a second chunk ahead
+      // measured slower: 29.6 against 23.0 ms on RMAT-24)
+      uint64_t c = tk.z + wib;
+      uint4 dd;
+      uint2 rr;
+      uint32_t r0;
+      bin_load_chunk(a, c, tk.w, lane, dd, rr, r0);
+      for (; c < tk.w; c += kW) {
+        uint4 ddn;
+        uint2 rrn;
+        uint32_t r0n;
+        bin_load_chunk(a, c + kW, tk.w, lane, ddn, rrn, r0n);
+        float x[8];
+        bin_load_vals(a, c_in, dd, rr, r0, x);
+        bin_add(s_sum, dd, x);
+        dd = ddn;
+        rr = rrn;
+        r0 = r0n;
+      }
+      __syncthreads();
+      for (uint32_t d = tid; d < nv; d += BLOCK) {
+        const float x = s_sum[d];
+        if (!multi) acc_cur[v0 + d] = x;
+        else if (x != 0.f) atomicAdd(&acc_cur[v0 + d], x);
+      }
+      __syncthreads();  // s_sum and s_task are reused by the next task
+    }
 }
 
 template <int BLOCK>
@@ -551,47 +601,7 @@ __global__ void __launch_bounds__(BLOCK, 1) pr_pull_binned(PrArgs a) {
       clear_change(ctl, (it + 1) % 3);
       ctl->task_next[(it + 1) & 1] = 0u;  // the counter iteration it + 1 takes (it - 1's is done)
     }
-    // ---- gather -----------------------------------------------------------------
-    for (;;) {
-      if (tid == 0) s_task = atomicAdd(&ctl->task_next[it & 1], 1u);
-      __syncthreads();
-      const uint32_t t = s_task;
-      if (t >= a.b_ntasks) break;  // uniform
-      const uint4 tk = ldg(a.b_tasks + t);
-      const uint32_t v0 = tk.x, nv = tk.y & 0x7FFFFFFFu;
-      const bool multi = (tk.y >> 31) != 0u;
-      for (uint32_t d = tid; d < nv; d += BLOCK) s_sum[d] = 0.f;
-      __syncthreads();
-      // a lane takes 8 consecutive arcs of a chunk (sorted by destination
-      // inside the chunk, so equal destinations are summed in registers
-      // before one shared-memory atomic); the next chunk's words load while
-      // this chunk's contributions are read and added (a second chunk ahead
-      // measured slower: 29.6 against 23.0 ms on RMAT-24)
-      uint64_t c = tk.z + wib;
-      uint4 dd;
-      uint2 rr;
-      uint32_t r0;
-      bin_load_chunk(a, c, tk.w, lane, dd, rr, r0);
-      for (; c < tk.w; c += kW) {
-        uint4 ddn;
-        uint2 rrn;
-        uint32_t r0n;
-        bin_load_chunk(a, c + kW, tk.w, lane, ddn, rrn, r0n);
-        float x[8];
-        bin_load_vals(a, c_io, dd, rr, r0, x);
-        bin_add(s_sum, dd, x);
-        dd = ddn;
-        rr = rrn;
-        r0 = r0n;
-      }
-      __syncthreads();
-      for (uint32_t d = tid; d < nv; d += BLOCK) {
-        const float x = s_sum[d];
-        if (!multi) acc_cur[v0 + d] = x;
-        else if (x != 0.f) atomicAdd(&acc_cur[v0 + d], x);
-      }
-      __syncthreads();  // s_sum and s_task are reused by the next task
-    }
+    bin_gather<BLOCK>(a, c_io, acc_cur, it, s_sum, &s_task);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     // ---- finish: ranks and contributions for the next gather
     double my_l1 = 0.0;
@@ -776,6 +786,62 @@ __global__ void __launch_bounds__(kBlock) pr_pull_residual_persistent(PrArgs a) 
       a.acc[v] = 0.f;
       finish(v, sum);
     }
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    const uint32_t accum = *reinterpret_cast<volatile uint32_t*>(&ctl->active[it % 3]);
+    if (gtid == 0) ctl->iters = it + 1;
+    if (it + 1 >= a.max_iter || accum == 0) break;
+  }
+}
+
+// Pull-residual rounds over the binned layout (degree-ordered graphs): the
+// vertex pass of round it first closes round it - 1 (a positive sum becomes
+// the residual), then takes the residuals above tol (value += residual,
+// delta = residual * alpha / outdeg), and the gather sums the deltas over
+// the in-arcs.  The rounds, their deltas and the stopping rule are those of
+// pr_pull_residual_persistent; a round ends in two grid barriers, not three.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1) pr_resid_binned(PrArgs a) {
+  extern __shared__ float s_sum[];  // kBinPart floats
+  __shared__ uint32_t s_task;
+  PrCtl* ctl = a.ctl;
+  const uint64_t deadline = kernel_deadline();
+  const uint64_t gtid = blockIdx.x * (uint64_t)BLOCK + threadIdx.x;
+  const uint64_t gthreads = (uint64_t)gridDim.x * BLOCK;
+  for (uint32_t it = 0;; ++it) {
+    float* const acc_prev = (it & 1) ? a.acc : a.acc2;  // round it - 1's sums
+    float* const acc_cur = (it & 1) ? a.acc2 : a.acc;
+    if (gtid == 0) {
+      ctl->active[(it + 1) % 3] = 0;
+      ctl->task_next[(it + 1) & 1] = 0u;
+    }
+    uint32_t my_accum = 0;
+    for (uint64_t v = gtid; v < a.n; v += gthreads) {
+      float r = a.residual[v];
+      if (it > 0) {
+        const float sum = acc_prev[v];
+        if (sum > 0.f) r = sum;
+      }
+      // the sums of round it - 2, read by round it - 1: zeroed for this
+      // round's gather (zeroing the slots the last gather's atomics just
+      // updated stalls)
+      acc_cur[v] = 0.f;
+      float d = 0.f;
+      if (r > a.tol) {
+        a.value[v] += r;
+        const uint32_t k = a.nout[v];
+        if (k > 0) {
+          d = r * a.alpha / (float)k;
+          ++my_accum;
+        }
+        r = 0.f;
+      }
+      a.residual[v] = r;
+      a.delta[v] = d;
+    }
+    my_accum = __reduce_add_sync(kFull, my_accum);
+    if (lane_id() == 0 && my_accum) atomicAdd(&ctl->active[it % 3], my_accum);
+    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    bin_gather<BLOCK>(a, a.delta, acc_cur, it, s_sum, &s_task);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
     const uint32_t accum = *reinterpret_cast<volatile uint32_t*>(&ctl->active[it % 3]);
     if (gtid == 0) ctl->iters = it + 1;
@@ -1286,6 +1352,24 @@ int run_pagerank(gb_graph* g, PrKind kind, float alpha, float tol, uint32_t max_
     pr_resid_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     GB_CUDA(cudaMemsetAsync(a.acc, 0, sizeof(float) * n, s));
     kfn = reinterpret_cast<const void*>(&pr_pull_residual_persistent);
+    if (g->perm && (g->order == GB_ORDER_DEGREE || g->order == GB_ORDER_DEGREE_UNSORTED)) {
+      if (ensure_pr_bins(g, s) == GB_OK) {  // else the row sweep
+        const PrBins* b = g->prb;
+        a.b_dst = b->dst;
+        a.b_roff = b->roff;
+        a.b_crun = b->crun;
+        a.b_rsrc = b->rsrc;
+        a.b_tasks = b->tasks;
+        a.b_ntasks = b->ntasks;
+        GB_CUDA(cudaMemsetAsync(a.acc2, 0, sizeof(float) * n, s));
+        kfn = reinterpret_cast<const void*>(&pr_resid_binned<kBinBlock>);
+        block = kBinBlock;
+        smem = sizeof(float) * kBinPart;
+        GB_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      } else {
+        clear_error();
+      }
+    }
   } else if (kind == PrKind::Push) {
     pr_push_init<<<g->sm_count * 4, 256, 0, s>>>(a);
     kfn = reinterpret_cast<const void*>(&pr_push_persistent);
