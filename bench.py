@@ -902,8 +902,9 @@ def roofline_of(job: Job, r: dict, order: int, traffic) -> dict:
     peak, peak_src = measured_peak_hbm()
     sec = sum(r["kms"]) / 1e3
     kernel = job.kernel
-    if type(job) is PrJob and 1 in r["orders"]:
-        kernel = "pr_pull_binned"  # a degree-ordered PageRank runs the binned pull kernel
+    if isinstance(job, PrJob) and 1 in r["orders"]:
+        # a degree-ordered PageRank runs the binned kernels
+        kernel = "pr_resid_binned" if isinstance(job, PrResidualJob) else "pr_pull_binned"
     elif type(job) is SsspJob:
         # the region kernel reports its shared-memory rounds in pull_rounds
         kernel = " + ".join(f"{'sssp_region' if st.get('pull_rounds') else 'sssp_persistent'} ({g['name']})"
