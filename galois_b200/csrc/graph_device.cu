@@ -408,8 +408,8 @@ int gb_graph_free(gb_graph* g) {
   cudaFree(g->colsum);
   cudaFree(g->ell);
   if (g->ppr_free) g->ppr_free(g);
-  cudaFree(g->sweep_tiles);
-  cudaFree(g->sweep_heavy_list);
+  pool_free(g->sweep_tiles);
+  pool_free(g->sweep_heavy_list);
   cudaFree(g->mg_first);
   cudaFree(g->mg_src);
   cudaFree(g->mg_level);

@@ -217,8 +217,8 @@ void drop_derived(gb_graph* g) {
   g->ell = nullptr;
   g->ell_d = 0;
   g->region_arcs = 0;
-  cudaFree(g->sweep_tiles);
-  cudaFree(g->sweep_heavy_list);
+  pool_free(g->sweep_tiles);
+  pool_free(g->sweep_heavy_list);
   g->sweep_tiles = nullptr;
   g->sweep_heavy_list = nullptr;
   g->sweep_ntiles = g->sweep_nheavy = g->sweep_heavy = g->sweep_tile = 0;

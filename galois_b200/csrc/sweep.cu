@@ -53,17 +53,21 @@ int build_row_schedule(const uint64_t* offs, uint32_t n, uint64_t m, uint32_t he
 
 int ensure_sweep_schedule(gb_graph* g, uint32_t heavy, uint32_t tile, cudaStream_t s, SweepSched* out) {
   if (!(g->sweep_tiles && g->sweep_heavy == heavy && g->sweep_tile == tile)) {
-    cudaFree(g->sweep_tiles);
-    cudaFree(g->sweep_heavy_list);
+    // pooled (graph_device.cu): a one-shot graph's upload / query / free
+    // cycle then makes no cudaMalloc or cudaFree, whose cost varied from
+    // under 1 ms to over 600 ms between calls on a loaded host
+    if (g->sweep_tiles) GB_CUDA(cudaStreamSynchronize(s));  // a kernel on s may still read the old schedule
+    pool_free(g->sweep_tiles);
+    pool_free(g->sweep_heavy_list);
     g->sweep_tiles = nullptr;
     g->sweep_heavy_list = nullptr;
     const uint64_t tc64 = g->m / tile + g->m / ((uint64_t)heavy + 1) + 2;
     const uint32_t tile_cap = (uint32_t)std::min<uint64_t>(tc64, 0xFFFFFFF0ull);
     const uint32_t heavy_cap = (uint32_t)std::min<uint64_t>(g->m / ((uint64_t)heavy + 1) + 2, 0xFFFFFFF0ull);
-    GB_CUDA(cudaMalloc(&g->sweep_tiles, sizeof(uint2) * tile_cap));
-    GB_CUDA(cudaMalloc(&g->sweep_heavy_list, sizeof(uint32_t) * heavy_cap));
+    GB_CUDA(pool_malloc(reinterpret_cast<void**>(&g->sweep_tiles), sizeof(uint2) * tile_cap));
+    GB_CUDA(pool_malloc(reinterpret_cast<void**>(&g->sweep_heavy_list), sizeof(uint32_t) * heavy_cap));
     uint32_t* dcount = nullptr;
-    GB_CUDA(cudaMalloc(&dcount, 16));
+    GB_CUDA(pool_malloc(reinterpret_cast<void**>(&dcount), 16));
     GB_CUDA(cudaMemsetAsync(dcount, 0, 16, s));
     sweep_tiles_kernel<<<g->sm_count * 4, 256, 0, s>>>(g->offs, g->n, heavy, tile, g->sweep_tiles, tile_cap,
                                                         g->sweep_heavy_list, heavy_cap, dcount,
@@ -71,7 +75,7 @@ int ensure_sweep_schedule(gb_graph* g, uint32_t heavy, uint32_t tile, cudaStream
     uint32_t* h = static_cast<uint32_t*>(g->pinned);
     cudaMemcpyAsync(h, dcount, 16, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
-    cudaFree(dcount);
+    pool_free(dcount);
     if (e != cudaSuccess) return cuda_fail(e, "sweep schedule");
     if (h[2]) GB_FAIL(GB_ERR_CAPACITY, "sweep schedule overflow");
     g->sweep_ntiles = h[0];
