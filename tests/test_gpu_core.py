@@ -385,6 +385,54 @@ def test_pagerank_residual_vs_restatement(cuda_device, name, method, restated, s
     assert abs(st["iterations"] - it64) <= 2, f"{name}: {st['iterations']} rounds vs {it64}"
 
 
+def _star_with_path(k, plen):
+    """A star of k leaves (one hub with k arcs each way) plus a detached path."""
+    s = [0] * k + list(range(1, k + 1)) + list(range(k + 1, k + plen)) + list(range(k + 2, k + plen + 1))
+    d = list(range(1, k + 1)) + [0] * k + list(range(k + 2, k + plen + 1)) + list(range(k + 1, k + plen))
+    return HostCSR.from_edges(k + plen + 1, s, d)
+
+
+@pytest.mark.parametrize("case", ["hub-split", "directed", "single-partition", "many-partitions"])
+def test_pagerank_binned_layout(cuda_device, case):
+    """Degree-ordered graphs run PageRank pull and pull-residual over the
+    binned layout (partitions of 32 768 destinations, 256-arc chunks).
+    Shapes that exercise it: a hub whose partition is split over several
+    tasks (sums added with atomics), a directed graph with rows that have no
+    arcs but sources that do, a graph smaller than one partition, and one of
+    several partitions.  Pull against the FP64 Jacobi oracle (<= 1e-5,
+    iterations within 2) and against the file-order row sweep (<= 1e-6);
+    pull-residual against the FP64 restatement of its rounds
+    (check_residual_parity, rounds within 2)."""
+    tol = 1e-6
+    if case == "hub-split":
+        # fp32 Jacobi on a 150 K-leaf star settles into a rounding limit cycle
+        # whose L1 change stays near 2-3e-6 (the row sweep's near 3e-6 to 2e-5):
+        # a 1e-6 tolerance is never met there, by either kernel
+        g, sym = _star_with_path(150000, 3000), True
+        tol = 1e-5
+    elif case == "directed":
+        g, _ = rmat(14, 8, seed=5, symmetrize=False)
+        sym = False
+    elif case == "single-partition":
+        g, sym = grid2d(100, 120), True
+    else:
+        g, _ = rmat(17, 8, seed=6)
+        sym = True
+    want, it64 = oracle.pr_pull_topo_f64(g, 0.85, tol, 1000)
+    with DeviceGraph(g, symmetric=sym) as plain:
+        ref = plain.pagerank_pull(0.85, tol, 1000)
+    with DeviceGraph(g, symmetric=sym, reorder=_lib.GB_ORDER_DEGREE) as dg:
+        for _ in range(2):  # the second call reuses the cached layout
+            got, st = dg.pagerank_pull(0.85, tol, 1000, stats=True)
+            assert np.max(np.abs(got.astype(np.float64) - want)) <= 1e-5, case
+            assert abs(st["iterations"] - it64) <= 2, (case, st["iterations"], it64)
+            assert np.max(np.abs(got - ref)) <= 1e-5, case
+        rwant, rit = oracle.pr_pull_residual(g, 0.85, 1e-4, 1000, f64=True)
+        rgot, rst = dg.pagerank_pull_residual(0.85, 1e-4, 1000, stats=True)
+        check_residual_parity(rgot, rwant, 1e-4, f"pull-residual {case}")
+        assert abs(rst["iterations"] - rit) <= 2, case
+
+
 @pytest.mark.parametrize("method,kw", [("pagerank_pull_residual", {}), ("pagerank_push", {}),
                                        ("pagerank_push", {"algo": "async"})])
 def test_pagerank_residual_converges_to_fixed_point(cuda_device, method, kw):
