@@ -49,7 +49,7 @@ struct gb_graph {
   // vertex, columns then uint32 weights, empty slots 0xFFFFFFFF), for SSSP
   uint32_t* ell = nullptr;
   uint32_t ell_d = 0;
-  // largest arc count of a 4096-vertex region + 1 (0: not computed) and the
+  // largest arc count of an SSSP region (sssp.cu) + 1 (0: not computed) and the
   // fraction of arcs inside their region, for SSSP
   uint64_t region_arcs = 0;
   double region_local = 0.0;

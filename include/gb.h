@@ -243,18 +243,18 @@ typedef struct gb_tuning {
   float do_beta;         /* pull->push switch (bfsDirectionOpt.cpp:73-77)  */
   int direction_opt;     /* 0 = pull steps allowed when in-edges exist, 2 = push only */
   int local_depth;       /* SSSP: per-warp local-queue rounds per phase
-                            (0 = library default, < 0 = off); with
-                            sssp_async = 3, shared-memory rounds between
-                            flushes of a region's outgoing relaxations */
+                            (0 = library default, < 0 = off); the region
+                            kernel flushes a region's outgoing relaxations
+                            every local_depth / 2 shared-memory rounds */
   int sssp_async;        /* SSSP with local queues on a graph whose every
                             vertex is light: 1 = asynchronous buckets (no
                             grid barrier inside a bucket), 2 = the same over
                             fixed-width rows when the degree is <= 8 (one
                             memory round trip per hop: faster on narrow,
                             chain-like graphs, slower on wide wavefronts);
-                            3 = regions of 4096 consecutive ids relaxed in
+                            3 = regions of 2048 consecutive ids relaxed in
                             shared memory when every region holds at most
-                            16384 arcs (for graphs numbered by locality,
+                            8192 arcs (for graphs numbered by locality,
                             GB_ORDER_LOCALITY; otherwise as 1); stats:
                             rounds = region visits, pull_rounds =
                             shared-memory rounds;

@@ -232,7 +232,7 @@ def test_sssp_async_small_ring_and_blocks(cuda_device):
 
 @pytest.mark.parametrize("shift", [13, 8, 0])
 def test_sssp_regions_bit_exact(cuda_device, shift):
-    """Regions of 4096 consecutive ids relaxed in shared memory (tuning
+    """Regions of 2048 consecutive ids relaxed in shared memory (tuning
     sssp_async = 3) against Dijkstra: grids of many regions in file order and
     in locality order (compact regions), a ragged last region, an
     unreachable part, and a grid whose regions hold too many arcs (8
