@@ -945,10 +945,14 @@ struct RegionArgs {
   uint32_t nregions;
 };
 
+// D = 0: the region's arcs as CSR (row offsets, columns, weights); D > 0:
+// fixed rows of D slots per vertex (graphs of degree <= D: a lane reads its
+// arc from the vertex id alone, one dependent load fewer per round).
+template <int D>
 constexpr size_t region_smem_bytes() {
-  return sizeof(uint32_t) * kRegion              // distances
-         + sizeof(uint32_t) * (kRegion + 4)      // local row offsets
-         + 2 * sizeof(uint32_t) * kRegionArcs    // columns, weights
+  return sizeof(uint32_t) * kRegion                                    // distances
+         + (D ? 0 : sizeof(uint32_t) * (kRegion + 4))                  // local row offsets
+         + 2 * sizeof(uint32_t) * (D ? (size_t)kRegion * D : kRegionArcs)  // columns, weights
          + 2 * sizeof(uint16_t) * kRegion        // the two round worklists
          + 3 * sizeof(uint32_t) * (kRegion / 32) // two listed bitmaps, pending words taken
          + sizeof(uint2) * kRegionOut;           // outbox
@@ -1081,16 +1085,39 @@ __device__ __forceinline__ void region_load(const SsspArgs& a, uint32_t base, ui
   }
 }
 
+// The region's distances, and its arcs as rows of D slots (empty slots
+// kNoArc; every vertex has at most D arcs, checked on the host).
+template <int D>
+__device__ __forceinline__ void region_load_rows(const SsspArgs& a, uint32_t base, uint32_t nv, uint32_t* s_dist,
+                                                 uint32_t* s_col, uint32_t* s_w) {
+  const uint32_t tid = threadIdx.x;
+  const uint4* d4 = reinterpret_cast<const uint4*>(a.dist + base);
+#pragma unroll 4
+  for (uint32_t q = tid; q < nv / 4; q += kRegionBlock) reinterpret_cast<uint4*>(s_dist)[q] = __ldcg(d4 + q);
+  for (uint32_t i = (nv & ~3u) + tid; i < nv; i += kRegionBlock) s_dist[i] = __ldcg(a.dist + base + i);
+  for (uint32_t lv = tid; lv < nv; lv += kRegionBlock) {
+    const uint64_t b = ldg(a.offs + base + lv), e = ldg(a.offs + base + lv + 1);
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      const bool ok = b + k < e;
+      s_col[lv * D + k] = ok ? ldg(a.col + b + k) : kNoArc;
+      s_w[lv * D + k] = ok ? ldg(a.w + b + k) : 0u;
+    }
+  }
+}
+
 // Needs every region's arcs to fit (at most kRegionArcs; checked on the host).
+template <int D>
 __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspArgs a, RegionArgs ra) {
   static_assert(worklists::kErrTimeout == kDevTimeout && worklists::kErrOverflow == kDevOverflow,
                 "the worklist raises the library's device error codes");
   extern __shared__ __align__(16) unsigned char s_raw[];
+  constexpr uint32_t kArcSlots = D ? kRegion * D : kRegionArcs;
   uint32_t* s_dist = reinterpret_cast<uint32_t*>(s_raw);
-  uint32_t* s_loff = s_dist + kRegion;
-  uint32_t* s_col = s_loff + kRegion + 4;
-  uint32_t* s_w = s_col + kRegionArcs;
-  uint2* s_out = reinterpret_cast<uint2*>(s_w + kRegionArcs);
+  uint32_t* s_loff = s_dist + kRegion;  // D == 0 only
+  uint32_t* s_col = D ? s_dist + kRegion : s_loff + kRegion + 4;
+  uint32_t* s_w = s_col + kArcSlots;
+  uint2* s_out = reinterpret_cast<uint2*>(s_w + kArcSlots);
   uint32_t* s_bm = reinterpret_cast<uint32_t*>(s_out + kRegionOut);  // [2][kRegion / 32] listed bitmaps
   uint32_t* s_pw = s_bm + 2 * (kRegion / 32);                          // pending words taken
   uint16_t* s_wl = reinterpret_cast<uint16_t*>(s_pw + kRegion / 32);   // [2][kRegion] round lists
@@ -1156,7 +1183,8 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
       }
       __threadfence();
       __syncthreads();
-      region_load(a, base, nv, o0, na, s_dist, s_loff, s_col, s_w);
+      if constexpr (D == 0) region_load(a, base, nv, o0, na, s_dist, s_loff, s_col, s_w);
+      else region_load_rows<D>(a, base, nv, s_dist, s_col, s_w);
       __syncthreads();
       // Round k relaxes list k & 1 (count s_n[k % 3]) into list (k + 1) & 1
       // (count s_n[(k + 1) % 3], listed bitmap (k + 1) & 1) and clears
@@ -1186,19 +1214,17 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
           const uint32_t v = has ? (uint32_t)wl[i] : 0u;
           const uint32_t d = has ? *reinterpret_cast<volatile uint32_t*>(&s_dist[v]) : hi;
           const bool live = d < hi;
-          uint32_t j = live ? s_loff[v] + sub : 0u;
-          const uint32_t e1 = live ? s_loff[v + 1] : 0u;
-          while (__any_sync(kFull, j < e1)) {
+          // relax one arc per lane (valid lanes), then the warp's appends;
+          // all lanes call
+          auto relax = [&](bool valid, uint32_t u, uint32_t nd, bool precheck) {
             bool to_next = false, to_out = false;
-            uint32_t u = 0, lu = 0, nd = 0;
-            if (j < e1) {
-              u = s_col[j];
-              nd = d + s_w[j];
-              j += 4;
+            uint32_t lu = 0;
+            if (valid) {
               ++my_scanned;
               lu = u - base;
               if (lu < nv) {
-                if (nd < *reinterpret_cast<volatile uint32_t*>(&s_dist[lu]) && nd < atomicMin(&s_dist[lu], nd)) {
+                if ((!precheck || nd < *reinterpret_cast<volatile uint32_t*>(&s_dist[lu])) &&
+                    nd < atomicMin(&s_dist[lu], nd)) {
                   ++my_relax;
                   const uint32_t bit = 1u << (lu & 31);
                   to_next = nd < hi && !(atomicOr(&bm_next[lu >> 5], bit) & bit);
@@ -1232,6 +1258,25 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
                 }
               }
             }
+          };
+          if constexpr (D == 0) {
+            uint32_t j = live ? s_loff[v] + sub : 0u;
+            const uint32_t e1 = live ? s_loff[v + 1] : 0u;
+            while (__any_sync(kFull, j < e1)) {
+              const bool ok = j < e1;
+              uint32_t u = 0, nd = 0;
+              if (ok) {
+                u = s_col[j];
+                nd = d + s_w[j];
+                j += 4;
+              }
+              relax(ok, u, nd, true);
+            }
+          } else {
+            // lane sub takes slot sub of the vertex's row (D == 4: one each)
+            static_assert(D == 4, "rows of 4 slots: one per lane of the group");
+            const uint32_t u = s_col[v * D + sub];
+            relax(live && u != kNoArc, u, d + s_w[v * D + sub], false);
           }
         }
         __syncthreads();
@@ -1453,8 +1498,10 @@ static int run_sssp_region(gb_graph* g, uint32_t src, uint32_t shift, int flush_
   GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(worklists::RingCtl), s));
   sssp_region_init<<<g->sm_count * 4, 256, 0, s>>>(a, ra);
   GB_CUDA(cudaGetLastError());
-  const void* kfn = reinterpret_cast<const void*>(&sssp_region);
-  const size_t smem = region_smem_bytes();
+  // graphs of degree <= 4 keep their arcs as 4-slot rows in shared memory
+  const bool rows = g->max_degree <= 4;
+  const void* kfn = rows ? reinterpret_cast<const void*>(&sssp_region<4>) : reinterpret_cast<const void*>(&sssp_region<0>);
+  const size_t smem = rows ? region_smem_bytes<4>() : region_smem_bytes<0>();
   GB_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = coop_grid(g, kfn, kRegionBlock, smem, kRegionPerSm);
   if (grid <= 0) GB_FAIL(GB_ERR_CUDA, "gb_sssp_delta: cannot size cooperative grid");
