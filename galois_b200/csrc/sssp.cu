@@ -1181,7 +1181,9 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
           for (uint32_t k = 0; bits; ++k, bits &= bits - 1) s_wl[pos + k] = (uint16_t)(j * 32 + __ffs(bits) - 1);
         }
       }
-      __threadfence();
+      // no fence: the exchanges above have returned, and a writer's
+      // atomicMin on a distance had returned before it set the pending bit
+      // (region_touch), so the L2 reads below (ldcg) see it
       __syncthreads();
       if constexpr (D == 0) region_load(a, base, nv, o0, na, s_dist, s_loff, s_col, s_w);
       else region_load_rows<D>(a, base, nv, s_dist, s_col, s_w);
@@ -1302,8 +1304,7 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
             }
           }
         }
-        __threadfence();
-        __syncthreads();
+        __syncthreads();  // (no fence: as at the visit's start)
         if (tid == 0) s_nout = 0;
         for (uint32_t i = tid; i < nv; i += kRegionBlock) {
           if (!((s_pw[i >> 5] >> (i & 31)) & 1u)) continue;
@@ -1330,10 +1331,8 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
       }
       __syncthreads();
       // release: vertices lowered from outside meanwhile queue the region again
-      if (tid == 0) {
-        __threadfence();
-        atomicExch(&ra.rq[r], 0u);
-      }
+      // the write-back atomics above have returned: the next visit's loads see them
+      if (tid == 0) atomicExch(&ra.rq[r], 0u);
       __syncthreads();
       if (tid < 32) {
         bool any = false;
