@@ -934,10 +934,11 @@ __global__ void __launch_bounds__(BLOCK) sssp_async_ell(SsspArgs a, const uint32
 // 29.3 ms for 4096 (one per SM) and 28.7 ms for 1024 (four per SM)
 constexpr uint32_t kRegion = 2048;       // vertices per region (a multiple of 32)
 constexpr uint32_t kRegionArcs = 8192;   // arcs a region may hold in shared memory
-constexpr uint32_t kRegionOut = 1024;    // outbox: relaxations of arcs leaving the region
+constexpr uint32_t kRegionOut = 128;     // outbox: relaxations of arcs leaving the region, per round
+constexpr uint32_t kRegionOutBufs = 8;   // outbox buffers (round k uses buffer k % 8)
 constexpr int kRegionBlock = 512;
 constexpr int kRegionPerSm = 2;
-constexpr uint32_t kRegionPoll = kRegion / 32;  // threads that poll the pending words during a flush
+constexpr int kRegionRelax = 448;        // threads that relax (warps 0-13); warps 14 and 15 are the couriers
 
 struct RegionArgs {
   uint32_t* pend;  // bitmap: vertex lowered from outside its region, to be expanded
@@ -954,8 +955,16 @@ constexpr size_t region_smem_bytes() {
          + (D ? 0 : sizeof(uint32_t) * (kRegion + 4))                  // local row offsets
          + 2 * sizeof(uint32_t) * (D ? (size_t)kRegion * D : kRegionArcs)  // columns, weights
          + 2 * sizeof(uint16_t) * kRegion        // the two round worklists
-         + 3 * sizeof(uint32_t) * (kRegion / 32) // two listed bitmaps, pending words taken
-         + sizeof(uint2) * kRegionOut;           // outbox
+         + 3 * sizeof(uint32_t) * (kRegion / 32) // two listed bitmaps, the inbox bitmap
+         + sizeof(uint2) * kRegionOutBufs * kRegionOut;  // outbox buffers
+}
+
+// Shared-memory flags between the relaxing warps and the couriers.
+__device__ __forceinline__ uint32_t ld_acquire_cta(uint32_t* p) {
+  return cuda::atomic_ref<uint32_t, cuda::thread_scope_block>(*p).load(cuda::memory_order_acquire);
+}
+__device__ __forceinline__ void st_release_cta(uint32_t* p, uint32_t v) {
+  cuda::atomic_ref<uint32_t, cuda::thread_scope_block>(*p).store(v, cuda::memory_order_release);
 }
 
 // Largest arc count of any region (out[0], the host check that regions fit)
@@ -1117,17 +1126,18 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
   uint32_t* s_loff = s_dist + kRegion;  // D == 0 only
   uint32_t* s_col = D ? s_dist + kRegion : s_loff + kRegion + 4;
   uint32_t* s_w = s_col + kArcSlots;
-  uint2* s_out = reinterpret_cast<uint2*>(s_w + kArcSlots);
-  uint32_t* s_bm = reinterpret_cast<uint32_t*>(s_out + kRegionOut);  // [2][kRegion / 32] listed bitmaps
-  uint32_t* s_pw = s_bm + 2 * (kRegion / 32);                          // pending words taken
-  uint16_t* s_wl = reinterpret_cast<uint16_t*>(s_pw + kRegion / 32);   // [2][kRegion] round lists
-  __shared__ uint32_t s_region, s_go, s_n[3], s_nout;
-  // rounds between outbox flushes: half the local depth (4 at its default of 8;
-  // flushing every 4 / 8 rounds measured 27.4 / 28.5 ms on the 4096^2 grid)
-  const uint32_t flush_every = a.local_depth > 1 ? (uint32_t)a.local_depth / 2 : 1u;
+  uint2* s_out = reinterpret_cast<uint2*>(s_w + kArcSlots);  // [kRegionOutBufs][kRegionOut] outbox
+  uint32_t* s_bm = reinterpret_cast<uint32_t*>(s_out + kRegionOutBufs * kRegionOut);  // [2][kRegion / 32] listed bitmaps
+  uint32_t* s_inbm = s_bm + 2 * (kRegion / 32);                         // inbox: taken pending vertices
+  uint16_t* s_wl = reinterpret_cast<uint16_t*>(s_inbm + kRegion / 32);  // [2][kRegion] round lists
+  // s_on: entries in each outbox buffer; s_obok[k & 1]: round k may use its
+  // buffer; s_opub: rounds published to the outbox courier; s_odone: rounds
+  // it has taken; s_qreq: the relaxers' latest request to finish; s_in_any:
+  // the inbox has vertices
+  __shared__ uint32_t s_region, s_go, s_n[3], s_on[kRegionOutBufs], s_obok[2], s_opub, s_odone, s_qreq, s_in_any;
   SsspCtl* ctl = a.ctl;
   worklists::RingCtl* rc = a.ring.rc;
-  const uint32_t tid = threadIdx.x, lane = lane_id();
+  const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
   const uint64_t deadline = kernel_deadline();
   const uint64_t gtid = blockIdx.x * (uint64_t)kRegionBlock + tid;
   const uint64_t gthreads = (uint64_t)gridDim.x * kRegionBlock;
@@ -1168,8 +1178,10 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
       const uint32_t nw = (nv + 31) >> 5;
       const uint64_t o0 = ldg(a.offs + base);
       const uint32_t na = (uint32_t)(ldg(a.offs + base + nv) - o0);
-      if (tid == 0) s_n[0] = s_n[1] = s_n[2] = s_nout = 0;
-      for (uint32_t j = tid; j < kRegion / 32; j += kRegionBlock) s_bm[kRegion / 32 + j] = 0u;
+      if (tid == 0) s_n[0] = s_n[1] = s_n[2] = s_opub = s_odone = s_qreq = s_in_any = 0;
+      if (tid < kRegionOutBufs) s_on[tid] = 0;
+      if (tid == 0) s_obok[0] = 1;
+      for (uint32_t j = tid; j < kRegion / 32; j += kRegionBlock) s_bm[kRegion / 32 + j] = s_inbm[j] = 0u;
       __syncthreads();
       // the pending vertices start the worklist; they are taken before the
       // distances are read, so a lowering after this point sets its bit again
@@ -1188,128 +1200,237 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
       if constexpr (D == 0) region_load(a, base, nv, o0, na, s_dist, s_loff, s_col, s_w);
       else region_load_rows<D>(a, base, nv, s_dist, s_col, s_w);
       __syncthreads();
-      // Round k relaxes list k & 1 (count s_n[k % 3]) into list (k + 1) & 1
-      // (count s_n[(k + 1) % 3], listed bitmap (k + 1) & 1) and clears
-      // bitmap k & 1 and s_n[(k + 2) % 3], which no thread uses in round k,
-      // so one CTA barrier per round suffices.  A vertex lowered while its
-      // entry is being expanded is listed again for the next round, so the
-      // expansion may read its distance at any time.  Four lanes share an
-      // entry, one arc each; each lane appends what it lists.  An arc that
-      // leaves the region goes to the outbox, flushed every `flush_every`
-      // rounds and when the list runs dry: the outbox into the global distances
-      // (queueing the targets' regions or filing them far) while threads
-      // 0-127 take this region's pending bits, whose vertices then join the
-      // next round.
-      uint32_t k = 0, since = 0;
-      for (;; ++k) {
-        const uint32_t cnt = s_n[k % 3];
-        const uint16_t* wl = s_wl + (k & 1) * kRegion;
-        uint16_t* wl_next = s_wl + ((k + 1) & 1) * kRegion;
-        uint32_t* bm_next = s_bm + ((k + 1) & 1) * (kRegion / 32);
-        uint32_t* n_next = &s_n[(k + 1) % 3];
-        if (tid == 0) s_n[(k + 2) % 3] = 0;
-        if (tid < kRegion / 32) s_bm[(k & 1) * (kRegion / 32) + tid] = 0u;
-        for (uint32_t i0 = (tid >> 5) * 8; i0 < cnt; i0 += kRegionBlock / 4) {  // warp-uniform
-          const uint32_t i = i0 + (lane >> 2), sub = lane & 3u;
-          const bool has = i < cnt;
-          const uint32_t v = has ? (uint32_t)wl[i] : 0u;
-          const uint32_t d = has ? *reinterpret_cast<volatile uint32_t*>(&s_dist[v]) : hi;
-          const bool live = d < hi;
-          // relax one arc per lane (valid lanes) and append what it lists
-          auto relax = [&](bool valid, uint32_t u, uint32_t nd, bool precheck) {
-            bool to_next = false, to_out = false;
-            uint32_t lu = 0;
-            if (valid) {
-              ++my_scanned;
-              lu = u - base;
-              if (lu < nv) {
-                if ((!precheck || nd < *reinterpret_cast<volatile uint32_t*>(&s_dist[lu])) &&
-                    nd < atomicMin(&s_dist[lu], nd)) {
-                  ++my_relax;
-                  const uint32_t bit = 1u << (lu & 31);
-                  to_next = nd < hi && !(atomicOr(&bm_next[lu >> 5], bit) & bit);
+      // Warps 0-13 relax in rounds.  Round k relaxes list k & 1 (count
+      // s_n[k % 3]) into list (k + 1) & 1 (count s_n[(k + 1) % 3], listed
+      // bitmap (k + 1) & 1) and clears bitmap k & 1 and s_n[(k + 2) % 3],
+      // which no thread uses in round k, so one barrier of the relaxing
+      // threads per round suffices.  A vertex lowered while its entry is
+      // being expanded is listed again for the next round, so the expansion
+      // may read its distance at any time.  Four lanes share an entry, one arc
+      // each; each lane appends what it lists.  An arc that leaves the region
+      // goes to outbox buffer k % 8, which warp 15 (a courier) applies to the
+      // global distances once the round is published (queueing the targets'
+      // regions or filing them far) while the rounds go on; when the courier
+      // has not yet taken the buffer's previous round, the arc is applied on
+      // the spot.  Warp 14 polls the region's pending bits: it takes them,
+      // lowers the shared distances to the global ones (atomicMin) and marks
+      // the vertices in the inbox bitmap.  Warps 12 and 13, which relax only
+      // in rounds of more than 96 entries, keep the books: warp 12 publishes
+      // the last round (a release), warp 13 clears the bitmap, moves the
+      // inbox into the next round's list and decides whether the next round
+      // may use its buffer (an acquire), so the fences (about 400 cycles
+      // each) stay off the other warps' path.  When a round lists nothing, the relaxers
+      // ask the couriers to finish (the outbox drained, one more poll) and all
+      // 512 threads meet; the visit goes on if the inbox holds vertices.
+      constexpr uint32_t kBooks = kRegionRelax / 32 - 1;  // the book-keeping warp
+      uint32_t k = 0, jo = 0;
+      for (uint32_t q = 1;; ++q) {
+        if (warp < kRegionRelax / 32) {
+          for (;; ++k) {
+            const uint32_t cnt = s_n[k % 3];
+            const uint16_t* wl = s_wl + (k & 1) * kRegion;
+            uint16_t* wl_next = s_wl + ((k + 1) & 1) * kRegion;
+            uint32_t* bm_next = s_bm + ((k + 1) & 1) * (kRegion / 32);
+            uint32_t* n_next = &s_n[(k + 1) % 3];
+            if (warp == kBooks - 1 && lane == 0) {
+              if (k > 0) st_release_cta(&s_opub, k);  // rounds < k are complete
+              s_n[(k + 2) % 3] = 0;
+            }
+            if (warp == kBooks) {
+              if (lane == 0) {
+                // round k + 1's buffer was last used by round k + 1 - 8 (none
+                // for k < 7); the courier clears its count when it takes it.
+                // (A count of zero is no sign: the courier may not have taken
+                // that empty round yet, and would read this round's count.)
+                const uint32_t nb = k + 1 - kRegionOutBufs;
+                const bool ok = k + 1 < kRegionOutBufs || ld_acquire_cta(&s_odone) > nb;
+                s_obok[(k + 1) & 1] = ok ? 1u : 0u;
+              }
+              s_bm[(k & 1) * (kRegion / 32) + lane] = 0u;
+              s_bm[(k & 1) * (kRegion / 32) + lane + 32] = 0u;
+              // the inbox flag is cleared before the bits are taken (the
+              // courier sets bits, then the flag)
+              uint32_t f = 0;
+              if (lane == 0 && *reinterpret_cast<volatile uint32_t*>(&s_in_any) != 0u) f = atomicExch(&s_in_any, 0u);
+              if (__shfl_sync(kFull, f, 0) != 0u) {
+                __threadfence_block();
+                for (uint32_t w = lane; w < nw; w += 32) {
+                  uint32_t bits = atomicExch(&s_inbm[w], 0u);
+                  for (; bits; bits &= bits - 1) {
+                    const uint32_t b = __ffs(bits) - 1, i = w * 32 + b;
+                    if (*reinterpret_cast<volatile uint32_t*>(&s_dist[i]) < hi &&
+                        !(atomicOr(&bm_next[w], 1u << b) & (1u << b)))
+                      wl_next[atomicAdd(n_next, 1u)] = (uint16_t)i;
+                  }
                 }
+              }
+            }
+            const bool ob_ok = *reinterpret_cast<volatile uint32_t*>(&s_obok[k & 1]) != 0u;
+            uint32_t* on = &s_on[k % kRegionOutBufs];
+            uint2* ob = s_out + (k % kRegionOutBufs) * kRegionOut;
+            for (uint32_t i0 = warp * 8; i0 < cnt; i0 += kRegionRelax / 4) {  // warp-uniform
+              const uint32_t i = i0 + (lane >> 2), sub = lane & 3u;
+              const bool has = i < cnt;
+              const uint32_t v = has ? (uint32_t)wl[i] : 0u;
+              const uint32_t d = has ? *reinterpret_cast<volatile uint32_t*>(&s_dist[v]) : hi;
+              const bool live = d < hi;
+              // relax one arc per lane (valid lanes) and append what it lists
+              auto relax = [&](bool valid, uint32_t u, uint32_t nd, bool precheck) {
+                if (!valid) return;
+                ++my_scanned;
+                const uint32_t lu = u - base;
+                if (lu < nv) {
+                  if ((!precheck || nd < *reinterpret_cast<volatile uint32_t*>(&s_dist[lu])) &&
+                      nd < atomicMin(&s_dist[lu], nd)) {
+                    ++my_relax;
+                    const uint32_t bit = 1u << (lu & 31);
+                    // each lane appends on its own: a shared-memory atomic on
+                    // the count is one dependent step, a warp-aggregated append
+                    // (vote, leader's atomic, shuffle) three
+                    if (nd < hi && !(atomicOr(&bm_next[lu >> 5], bit) & bit))
+                      wl_next[atomicAdd(n_next, 1u)] = (uint16_t)lu;
+                  }
+                  return;
+                }
+                if (ob_ok) {
+                  const uint32_t pos = atomicAdd(on, 1u);
+                  if (pos < kRegionOut) {
+                    ob[pos] = make_uint2(u, nd);
+                    return;
+                  }
+                }
+                if (nd < atomicMin(&a.dist[u], nd)) {  // no room: applied here
+                  ++my_relax;
+                  if (nd < hi) region_touch(a, ra, u, &ctl->err);
+                  else far_file(a, farq, far_count, u, &ctl->err);
+                }
+              };
+              if constexpr (D == 0) {
+                uint32_t j = live ? s_loff[v] + sub : 0u;
+                const uint32_t e1 = live ? s_loff[v + 1] : 0u;
+                for (; j < e1; j += 4) relax(true, s_col[j], d + s_w[j], true);
               } else {
-                to_out = true;
+                // lane sub takes slot sub of the vertex's row (D == 4: one each)
+                static_assert(D == 4, "rows of 4 slots: one per lane of the group");
+                const uint32_t u = s_col[v * D + sub];
+                relax(live && u != kNoArc, u, d + s_w[v * D + sub], false);
               }
             }
-            // appends by each lane on its own: a shared-memory atomic on the
-            // count is one dependent step, the warp-aggregated form (vote,
-            // leader's atomic, shuffle) three (grid 23.2 -> 21.0 ms)
-            if (to_next) wl_next[atomicAdd(n_next, 1u)] = (uint16_t)lu;
-            if (to_out) {
-              const uint32_t pos = atomicAdd(&s_nout, 1u);
-              if (pos < kRegionOut) {
-                s_out[pos] = make_uint2(u, nd);
-              } else if (nd < atomicMin(&a.dist[u], nd)) {  // outbox full
-                ++my_relax;
-                if (nd < hi) region_touch(a, ra, u, &ctl->err);
-                else far_file(a, farq, far_count, u, &ctl->err);
-              }
-            }
-          };
-          if constexpr (D == 0) {
-            uint32_t j = live ? s_loff[v] + sub : 0u;
-            const uint32_t e1 = live ? s_loff[v + 1] : 0u;
-            while (__any_sync(kFull, j < e1)) {
-              const bool ok = j < e1;
-              uint32_t u = 0, nd = 0;
-              if (ok) {
-                u = s_col[j];
-                nd = d + s_w[j];
-                j += 4;
-              }
-              relax(ok, u, nd, true);
-            }
-          } else {
-            // lane sub takes slot sub of the vertex's row (D == 4: one each)
-            static_assert(D == 4, "rows of 4 slots: one per lane of the group");
-            const uint32_t u = s_col[v * D + sub];
-            relax(live && u != kNoArc, u, d + s_w[v * D + sub], false);
+            asm volatile("bar.sync 1, %0;" ::"n"(kRegionRelax) : "memory");
+            // uniform: s_n[(k + 1) % 3] changes only after the next barrier
+            if (*n_next == 0) break;
           }
-        }
-        __syncthreads();
-        // uniform: s_n[(k + 1) % 3] changes only after the next barrier
-        if (*n_next != 0 && ++since < flush_every) continue;
-        since = 0;
-        if (tid < kRegionPoll) {
-          // take the pending bits before reading the distances they announce
-          uint32_t bits = 0;
-          if (tid < nw) {
-            bits = *reinterpret_cast<volatile uint32_t*>(&ra.pend[(base >> 5) + tid]);
-            if (bits) bits = atomicExch(&ra.pend[(base >> 5) + tid], 0u);
+          if (warp == kBooks && lane == 0) {
+            st_release_cta(&s_opub, k + 1);
+            st_release_cta(&s_qreq, q);
           }
-          s_pw[tid] = bits;
+          ++k;  // the next round (if the visit goes on) starts from an empty list
+        } else if (warp == kRegionRelax / 32) {
+          // pending courier: a pass that starts after the request is the last
+          const uint32_t pw0 = base >> 5;
+          for (uint32_t pass = 1;; ++pass) {
+            uint32_t qr = 0;
+            if (lane == 0) qr = ld_acquire_cta(&s_qreq);
+            qr = __shfl_sync(kFull, qr, 0);
+            uint32_t b0 = 0, b1 = 0;
+            if (lane < nw) {
+              b0 = *reinterpret_cast<volatile uint32_t*>(&ra.pend[pw0 + lane]);
+              if (b0) b0 = atomicExch(&ra.pend[pw0 + lane], 0u);
+            }
+            if (lane + 32 < nw) {
+              b1 = *reinterpret_cast<volatile uint32_t*>(&ra.pend[pw0 + lane + 32]);
+              if (b1) b1 = atomicExch(&ra.pend[pw0 + lane + 32], 0u);
+            }
+            // no fence: the exchanges have returned, and a writer's atomicMin
+            // had returned before it set the bit (region_touch)
+            bool any = false;
+            auto take_word = [&](uint32_t w, uint32_t bits) {
+              bool want = false;
+              if ((bits >> lane) & 1u) {
+                const uint32_t i = w * 32 + lane;
+                const uint32_t gd = __ldcg(a.dist + base + i);
+                // a bit asks for an expansion at the global distance: also
+                // when it equals the local one (read at the visit's start
+                // after the bit was set); a smaller local one is expanded
+                want = gd <= atomicMin(&s_dist[i], gd) && gd < hi;
+              }
+              const unsigned mk = __ballot_sync(kFull, want);
+              if (mk) {
+                any = true;
+                if (lane == 0) atomicOr(&s_inbm[w], mk);
+              }
+            };
+            for (unsigned m = __ballot_sync(kFull, b0 != 0u); m; m &= m - 1) {
+              const int src = __ffs(m) - 1;
+              take_word((uint32_t)src, __shfl_sync(kFull, b0, src));
+            }
+            for (unsigned m = __ballot_sync(kFull, b1 != 0u); m; m &= m - 1) {
+              const int src = __ffs(m) - 1;
+              take_word((uint32_t)src + 32, __shfl_sync(kFull, b1, src));
+            }
+            if (any && lane == 0) st_release_cta(&s_in_any, 1u);
+            if (qr == q) break;
+            if ((pass & 63u) == 0 && globaltimer_ns() > deadline) {
+              if (lane == 0) raise_err(&ctl->err, kDevTimeout);
+              break;
+            }
+          }
         } else {
-          const uint32_t no = min(s_nout, kRegionOut);
-          for (uint32_t i = tid - kRegionPoll; i < no; i += kRegionBlock - kRegionPoll) {
-            const uint2 o = s_out[i];
-            if (o.y < atomicMin(&a.dist[o.x], o.y)) {
-              ++my_relax;
-              if (o.y < hi) region_touch(a, ra, o.x, &ctl->err);
-              else far_file(a, farq, far_count, o.x, &ctl->err);
+          // outbox courier: every published round at once, then the request
+          for (uint32_t spins = 1;; ++spins) {
+            uint32_t qr = 0, pub = 0;
+            if (lane == 0) {
+              qr = ld_acquire_cta(&s_qreq);
+              pub = ld_acquire_cta(&s_opub);
+            }
+            qr = __shfl_sync(kFull, qr, 0);
+            pub = __shfl_sync(kFull, pub, 0);
+            if (jo < pub) {
+              // rounds [jo, pub): at most kRegionOutBufs of them are unread
+              // (a round uses its buffer only once the courier took it)
+              uint32_t total = 0;
+              uint32_t cum[kRegionOutBufs];
+#pragma unroll
+              for (uint32_t t = 0; t < kRegionOutBufs; ++t) {
+                const uint32_t r = jo + t;
+                const uint32_t c = r < pub ? min(*reinterpret_cast<volatile uint32_t*>(&s_on[r % kRegionOutBufs]), kRegionOut) : 0u;
+                total += c;
+                cum[t] = total;
+              }
+              for (uint32_t g = lane; g < total; g += 32) {
+                uint32_t t = 0, first = 0;
+#pragma unroll
+                for (uint32_t x = 0; x + 1 < kRegionOutBufs; ++x)
+                  if (g >= cum[x]) t = x + 1, first = cum[x];
+                const uint2 o = s_out[((jo + t) % kRegionOutBufs) * kRegionOut + (g - first)];
+                if (o.y < atomicMin(&a.dist[o.x], o.y)) {
+                  ++my_relax;
+                  if (o.y < hi) region_touch(a, ra, o.x, &ctl->err);
+                  else far_file(a, farq, far_count, o.x, &ctl->err);
+                }
+              }
+              __syncwarp();
+              const uint32_t nr = min(pub - jo, kRegionOutBufs);
+              if (lane < nr) s_on[(jo + lane) % kRegionOutBufs] = 0;
+              __syncwarp();
+              jo += nr;
+              if (lane == 0) st_release_cta(&s_odone, jo);
+              continue;
+            }
+            if (qr == q) break;  // read before pub: every round published before the request is taken
+            __nanosleep(32);
+            if ((spins & 255u) == 0 && globaltimer_ns() > deadline) {
+              if (lane == 0) raise_err(&ctl->err, kDevTimeout);
+              break;
             }
           }
         }
-        __syncthreads();  // (no fence: as at the visit's start)
-        if (tid == 0) s_nout = 0;
-        for (uint32_t i = tid; i < nv; i += kRegionBlock) {
-          if (!((s_pw[i >> 5] >> (i & 31)) & 1u)) continue;
-          // a bit asks for an expansion at the global distance: also when
-          // it equals the local one (the distance may have been read at the
-          // visit's start before its bit was set); a smaller local distance
-          // was lowered here and is expanded already
-          const uint32_t gd = __ldcg(a.dist + base + i);
-          if (gd <= s_dist[i]) {
-            s_dist[i] = gd;  // no relaxation runs during the flush
-            const uint32_t bit = 1u << (i & 31);
-            if (gd < hi && !(atomicOr(&bm_next[i >> 5], bit) & bit)) wl_next[atomicAdd(n_next, 1u)] = (uint16_t)i;
-          }
-        }
         __syncthreads();
-        if (*n_next == 0) break;
+        const bool go = *reinterpret_cast<volatile uint32_t*>(&s_in_any) != 0u;
+        __syncthreads();
+        if (!go) break;
       }
-      if (tid == 0) my_rounds += k + 1;
+      if (tid == 0) my_rounds += k;
       // write the lowered distances back; those beyond the bucket join the far pile
       for (uint32_t i = tid; i < nv; i += kRegionBlock) {
         const uint32_t d = s_dist[i];
@@ -1448,7 +1569,7 @@ static int finish_sssp(gb_graph* g, const SsspArgs& a, unsigned long long* reach
 }
 
 // The region kernel (every region's arcs fit in shared memory).
-static int run_sssp_region(gb_graph* g, uint32_t src, uint32_t shift, int flush_every, uint32_t nregions,
+static int run_sssp_region(gb_graph* g, uint32_t src, uint32_t shift, uint32_t nregions,
                            uint32_t* dist_out, bool out_dev, gb_stats* stats, cudaStream_t s) {
   const uint32_t n = g->n;
   const uint32_t words = (n + 31) / 32;
@@ -1479,7 +1600,6 @@ static int run_sssp_region(gb_graph* g, uint32_t src, uint32_t shift, int flush_
   a.src = src;
   a.shift = shift;
   a.max_phases = 0x7FFFFFFFu;
-  a.local_depth = flush_every;
   GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), s));
   GB_CUDA(cudaMemsetAsync(a.ring.rc, 0, sizeof(worklists::RingCtl), s));
   sssp_region_init<<<g->sm_count * 4, 256, 0, s>>>(a, ra);
@@ -1534,7 +1654,7 @@ int run_sssp(gb_graph* g, uint32_t src, uint32_t shift, uint32_t* dist_out, gb_s
     const bool fits = g->region_arcs - 1 <= kRegionArcs;
     region = t.sssp_async == 3 ? fits : fits && g->region_local >= 0.9;
   }
-  if (region) return run_sssp_region(g, src, shift, local_depth, nregions, dist_out, out_dev, stats, s);
+  if (region) return run_sssp_region(g, src, shift, nregions, dist_out, out_dev, stats, s);
   FrontierLayout fl = frontier_layout(n, g->m, t.heavy_degree, t.tile_edges);
   SweepSched sched{};
   if (!async && g->max_degree > t.heavy_degree) {  // heavy rows of a bitmap frontier come from the tile schedule

@@ -244,8 +244,7 @@ typedef struct gb_tuning {
   int direction_opt;     /* 0 = pull steps allowed when in-edges exist, 2 = push only */
   int local_depth;       /* SSSP: per-warp local-queue rounds per phase
                             (0 = library default, < 0 = off); the region
-                            kernel flushes a region's outgoing relaxations
-                            every local_depth / 2 shared-memory rounds */
+                            kernel does not use it */
   int sssp_async;        /* SSSP with local queues on a graph whose every
                             vertex is light: 1 = asynchronous buckets (no
                             grid barrier inside a bucket), 2 = the same over
