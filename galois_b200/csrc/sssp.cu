@@ -939,6 +939,7 @@ constexpr uint32_t kRegionOutBufs = 8;   // outbox buffers (round k uses buffer 
 constexpr int kRegionBlock = 512;
 constexpr int kRegionPerSm = 2;
 constexpr int kRegionRelax = 448;        // threads that relax (warps 0-13); warps 14 and 15 are the couriers
+static_assert(kRegion % kRegionBlock == 0, "a thread takes kRegion / kRegionBlock vertices of a region");
 
 struct RegionArgs {
   uint32_t* pend;  // bitmap: vertex lowered from outside its region, to be expanded
@@ -1104,13 +1105,26 @@ __device__ __forceinline__ void region_load_rows(const SsspArgs& a, uint32_t bas
 #pragma unroll 4
   for (uint32_t q = tid; q < nv / 4; q += kRegionBlock) reinterpret_cast<uint4*>(s_dist)[q] = __ldcg(d4 + q);
   for (uint32_t i = (nv & ~3u) + tid; i < nv; i += kRegionBlock) s_dist[i] = __ldcg(a.dist + base + i);
-  for (uint32_t lv = tid; lv < nv; lv += kRegionBlock) {
-    const uint64_t b = ldg(a.offs + base + lv), e = ldg(a.offs + base + lv + 1);
+  // a thread's vertices all at once: their offsets, then their arcs (two
+  // dependent loads in all, not two per vertex)
+  constexpr int kPer = kRegion / kRegionBlock;
+  uint64_t b[kPer], e[kPer];
 #pragma unroll
-    for (int k = 0; k < D; ++k) {
-      const bool ok = b + k < e;
-      s_col[lv * D + k] = ok ? ldg(a.col + b + k) : kNoArc;
-      s_w[lv * D + k] = ok ? ldg(a.w + b + k) : 0u;
+  for (int t = 0; t < kPer; ++t) {
+    const uint32_t lv = tid + t * kRegionBlock;
+    b[t] = e[t] = 0;
+    if (lv < nv) b[t] = ldg(a.offs + base + lv), e[t] = ldg(a.offs + base + lv + 1);
+  }
+#pragma unroll
+  for (int t = 0; t < kPer; ++t) {
+    const uint32_t lv = tid + t * kRegionBlock;
+    if (lv < nv) {
+#pragma unroll
+      for (int k = 0; k < D; ++k) {
+        const bool ok = b[t] + k < e[t];
+        s_col[lv * D + k] = ok ? ldg(a.col + b[t] + k) : kNoArc;
+        s_w[lv * D + k] = ok ? ldg(a.w + b[t] + k) : 0u;
+      }
     }
   }
 }
@@ -1161,7 +1175,8 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
         if (busy) atomicSub(&rc->work, 1);
         busy = false;
         const unsigned long long p = atomicAdd(&rc->head, 1ull);
-        const int got = worklists::wait_chunk(a.ring, p, &ctl->err, deadline);
+        // a queued region is on the path of the bucket's wave: poll often
+        const int got = worklists::wait_chunk(a.ring, p, &ctl->err, deadline, 128);
         s_go = got > 0 ? 1u : 0u;
         if (got > 0) {
           busy = true;  // the chunk's count is now this CTA's
@@ -1431,11 +1446,22 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
         if (!go) break;
       }
       if (tid == 0) my_rounds += k;
-      // write the lowered distances back; those beyond the bucket join the far pile
-      for (uint32_t i = tid; i < nv; i += kRegionBlock) {
-        const uint32_t d = s_dist[i];
-        if (d < __ldcg(a.dist + base + i) && d < atomicMin(&a.dist[base + i], d) && d >= hi)
-          far_file(a, farq, far_count, base + i, &ctl->err);
+      // write the lowered distances back (a thread's global distances read
+      // at once); those beyond the bucket join the far pile
+      {
+        constexpr int kPer = kRegion / kRegionBlock;
+        uint32_t gd[kPer];
+#pragma unroll
+        for (int t = 0; t < kPer; ++t) {
+          const uint32_t i = tid + t * kRegionBlock;
+          gd[t] = i < nv ? __ldcg(a.dist + base + i) : 0u;
+        }
+#pragma unroll
+        for (int t = 0; t < kPer; ++t) {
+          const uint32_t i = tid + t * kRegionBlock;
+          const uint32_t d = i < nv ? s_dist[i] : 0u;
+          if (d < gd[t] && d < atomicMin(&a.dist[base + i], d) && d >= hi) far_file(a, farq, far_count, base + i, &ctl->err);
+        }
       }
       __syncthreads();
       // release: vertices lowered from outside meanwhile queue the region again

@@ -173,14 +173,15 @@ __device__ __forceinline__ bool publish_one(const Ring& r, uint4 e, int* err) {
   }
   r.ent[slot * 32] = e;
   r.cnt[slot] = 1;
-  __threadfence();
-  st_release(r.seq + slot, p + 1);
+  st_release(r.seq + slot, p + 1);  // orders this thread's two stores before it
   return true;
 }
 
-// Lane 0 of a warp out of work: wait for the chunk of ring position p.
+// Lane 0 of a warp out of work: wait for the chunk of ring position p,
+// polling with a back-off that doubles from 32 ns up to max_ns.
 // 1: published; 0: no work left anywhere; -1: error (or deadline: raised).
-__device__ __forceinline__ int wait_chunk(const Ring& r, unsigned long long p, int* err, uint64_t deadline) {
+__device__ __forceinline__ int wait_chunk(const Ring& r, unsigned long long p, int* err, uint64_t deadline,
+                                          unsigned max_ns = 512) {
   const unsigned long long* sq = r.seq + (p & r.mask);
   unsigned spins = 0, ns = 32;
   for (;;) {
@@ -194,7 +195,7 @@ __device__ __forceinline__ int wait_chunk(const Ring& r, unsigned long long p, i
       }
     }
     __nanosleep(ns);
-    if (ns < 512) ns <<= 1;
+    if (ns < max_ns) ns <<= 1;
   }
 }
 
