@@ -100,6 +100,49 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int
   return s_ok != 0;
 }
 
+// grid_barrier whose last arriving CTA (its thread 0) runs last() before it
+// releases the others: a step that must see every CTA arrived and be seen by
+// every CTA after the barrier, without a second barrier.
+template <class F>
+__device__ __forceinline__ bool grid_barrier_last(GridBar* bar, unsigned nblocks, int* err, uint64_t deadline, F&& last,
+                                                  uint64_t timeout_ns = 2000000000ull) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0 && globaltimer_ns() > deadline) raise_err(err, kDevTimeout);
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(bar->gen);
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(bar->count);
+    const unsigned g = gen.load(cuda::memory_order_relaxed);
+    __threadfence();
+    const unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+    int ok = 1;
+    if (arrived == nblocks - 1) {
+      last();
+      cnt.store(0u, cuda::memory_order_relaxed);
+      gen.fetch_add(1u, cuda::memory_order_release);
+    } else {
+      const uint64_t t0 = globaltimer_ns();
+      unsigned spins = 0;
+      while (gen.load(cuda::memory_order_acquire) == g) {
+        if ((++spins & 31u) == 0) {
+          if (read_err(err)) { ok = 0; break; }
+          if (globaltimer_ns() - t0 > timeout_ns) {
+            raise_err(err, kDevTimeout);
+            ok = 0;
+            break;
+          }
+        }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+    if (ok && read_err(err)) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 // Append `item` for every lane with pred set; all 32 lanes must call.
 __device__ __forceinline__ void warp_push(bool pred, uint32_t item, uint32_t* queue,
                                           uint32_t* count, uint32_t cap, int* err) {

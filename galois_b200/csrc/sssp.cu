@@ -92,6 +92,8 @@ struct SsspCtl {
   unsigned long long scanned;
   unsigned long long relax;
   unsigned long long local_rounds;  // region kernel: shared-memory rounds over all visits
+  uint32_t far_min[2];              // region kernel: least bucket recorded for each far pile
+  uint32_t pad2[2];
 };
 
 struct SsspArgs {
@@ -1005,6 +1007,7 @@ __global__ void sssp_region_init(SsspArgs a, RegionArgs ra) {
   }
   const uint32_t r0 = a.src / kRegion;
   for (uint64_t r = tid; r < ra.nregions; r += stride) ra.rq[r] = (r == r0) ? 1u : 0u;
+  if (tid == 0) a.ctl->far_min[0] = a.ctl->far_min[1] = 0xFFFFFFFFu;
   for (uint64_t i = tid; i <= a.ring.mask; i += stride) {
     if (i == 0) {  // the source's region, published as the chunk of position 0 (counted in work)
       a.ring.ent[0] = make_uint4(r0, 0u, 0u, 0u);
@@ -1034,8 +1037,11 @@ __device__ __forceinline__ void region_touch(const SsspArgs& a, const RegionArgs
   if (atomicOr(&ra.rq[rg], 1u) == 0u) worklists::publish_one(a.ring, make_uint4(rg, 0u, 0u, 0u), err);
 }
 
-// File u (lowered to a distance beyond the bucket) in the far pile once.
-__device__ __forceinline__ void far_file(const SsspArgs& a, uint32_t* farq, uint32_t* count, uint32_t u, int* err) {
+// File u (lowered to nd, beyond the bucket) in the far pile once, and record
+// nd's bucket in the CTA's least bucket for the pile (s_fmin).
+__device__ __forceinline__ void far_file(const SsspArgs& a, uint32_t* farq, uint32_t* count, uint32_t u, uint32_t nd,
+                                         uint32_t* s_fmin, int* err) {
+  atomicMin(s_fmin, nd >> a.shift);
   const uint32_t bit = 1u << (u & 31);
   if (!(__ldcg(a.infar + (u >> 5)) & bit) && !(atomicOr(&a.infar[u >> 5], bit) & bit)) {
     const uint32_t pos = atomicAdd(count, 1u);
@@ -1149,6 +1155,10 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
   // it has taken; s_qreq: the relaxers' latest request to finish; s_in_any:
   // the inbox has vertices
   __shared__ uint32_t s_region, s_go, s_n[3], s_on[kRegionOutBufs], s_obok[2], s_opub, s_odone, s_qreq, s_in_any;
+  // least bucket of the distances this CTA filed in the current far pile
+  // since it last added them to ctl->far_min
+  __shared__ uint32_t s_fmin;
+  if (threadIdx.x == 0) s_fmin = 0xFFFFFFFFu;  // the first barrier below orders it
   SsspCtl* ctl = a.ctl;
   worklists::RingCtl* rc = a.ring.rc;
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
@@ -1317,7 +1327,7 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
                 if (nd < atomicMin(&a.dist[u], nd)) {  // no room: applied here
                   ++my_relax;
                   if (nd < hi) region_touch(a, ra, u, &ctl->err);
-                  else far_file(a, farq, far_count, u, &ctl->err);
+                  else far_file(a, farq, far_count, u, nd, &s_fmin, &ctl->err);
                 }
               };
               if constexpr (D == 0) {
@@ -1421,7 +1431,7 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
                 if (o.y < atomicMin(&a.dist[o.x], o.y)) {
                   ++my_relax;
                   if (o.y < hi) region_touch(a, ra, o.x, &ctl->err);
-                  else far_file(a, farq, far_count, o.x, &ctl->err);
+                  else far_file(a, farq, far_count, o.x, o.y, &s_fmin, &ctl->err);
                 }
               }
               __syncwarp();
@@ -1460,7 +1470,8 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
         for (int t = 0; t < kPer; ++t) {
           const uint32_t i = tid + t * kRegionBlock;
           const uint32_t d = i < nv ? s_dist[i] : 0u;
-          if (d < gd[t] && d < atomicMin(&a.dist[base + i], d) && d >= hi) far_file(a, farq, far_count, base + i, &ctl->err);
+          if (d < gd[t] && d < atomicMin(&a.dist[base + i], d) && d >= hi)
+            far_file(a, farq, far_count, base + i, d, &s_fmin, &ctl->err);
         }
       }
       __syncthreads();
@@ -1477,54 +1488,55 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
       }
       __syncthreads();
     }
-    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
-    // ---- bucket transition ---------------------------------------------------------
-    const uint32_t nfar = min(ctl->far_count[fp], a.n);
+    // ---- bucket transition: two grid barriers -------------------------------------
+    // The least bucket of the pile is recorded as entries are filed (and as
+    // R2 keeps them): every entry's distance was recorded when it was set,
+    // so the record is at most the least bucket still in the pile (a bucket
+    // emptied since by lowerings only costs an empty bucket).
+    if (tid == 0 && s_fmin != 0xFFFFFFFFu) {
+      atomicMin(&ctl->far_min[fp], s_fmin);
+      s_fmin = 0xFFFFFFFFu;
+    }
+    // the last CTA to arrive voids the tickets still waiting: no CTA waits any more
+    if (!grid_barrier_last(&ctl->bar, gridDim.x, &ctl->err, deadline, [&] { rc->head = rc->tail; })) return;
+    const uint32_t nfar = min(__ldcg(&ctl->far_count[fp]), a.n);
     ++P;
     if (nfar == 0) break;  // nothing left anywhere
-    if (gtid == 0) {
-      rc->head = rc->tail;  // tickets still waiting when the bucket ended are void
-      ctl->min_bucket = 0xFFFFFFFFu;
-      ctl->buckets += 1;
-      ctl->far_count[fp ^ 1] = 0;
-    }
-    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
-    // R1: minimum bucket among far entries not yet settled
-    {
-      uint32_t mb = 0xFFFFFFFFu;
-      for (uint64_t i = gtid; i < nfar; i += gthreads) {
-        const uint32_t dd = a.dist[farq[i]];
-        if (dd >= hi) mb = min(mb, dd >> a.shift);
-      }
-      mb = __reduce_min_sync(kFull, mb);
-      if (lane == 0 && mb != 0xFFFFFFFFu) atomicMin(&ctl->min_bucket, mb);
-    }
-    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
-    const uint32_t nb = ctl->min_bucket;
-    if (nb == 0xFFFFFFFFu) break;  // every far entry was settled
+    const uint32_t nb = __ldcg(&ctl->far_min[fp]);
+    if (nb == 0xFFFFFFFFu) break;  // nothing recorded: every far entry was settled
+    if (gtid == 0) ctl->buckets += 1;
     // R2: the entries of bucket nb become pending (their regions queued),
-    // later ones stay in the pile
+    // later ones stay in the pile (their buckets recorded for the next one)
     {
       const uint64_t nhi64 = ((uint64_t)nb + 1) << a.shift;
       const uint32_t nhi = nhi64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)nhi64;
       uint32_t* keepq = a.far[fp ^ 1];
+      uint32_t kmin = 0xFFFFFFFFu;
       for (uint64_t b0 = gtid - lane; b0 < nfar; b0 += gthreads) {
         const uint64_t i = b0 + lane;
         bool keep = false;
         uint32_t u = 0;
         if (i < nfar) {
           u = farq[i];
-          const uint32_t dd = a.dist[u];
+          const uint32_t dd = __ldcg(a.dist + u);
           if (dd >= hi && dd < nhi) region_touch(a, ra, u, &ctl->err);
-          else if (dd >= nhi) keep = true;
+          else if (dd >= nhi) keep = true, kmin = min(kmin, dd >> a.shift);
           if (!keep) atomicAnd(&a.infar[u >> 5], ~(1u << (u & 31)));
         }
         warp_push(keep, u, keepq, &ctl->far_count[fp ^ 1], a.n, &ctl->err);
       }
+      kmin = __reduce_min_sync(kFull, kmin);
+      if (lane == 0 && kmin != 0xFFFFFFFFu) atomicMin(&s_fmin, kmin);
     }
+    // the last CTA to arrive empties the pile just split
+    const int done_pile = fp;
+    if (!grid_barrier_last(&ctl->bar, gridDim.x, &ctl->err, deadline, [&] {
+          ctl->far_count[done_pile] = 0;
+          ctl->far_min[done_pile] = 0xFFFFFFFFu;
+        }))
+      return;
     bucket = nb;
     fp ^= 1;
-    if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
   }
   my_scanned = warp_sum(my_scanned);
   my_relax = warp_sum(my_relax);
