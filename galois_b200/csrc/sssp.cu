@@ -932,14 +932,17 @@ __global__ void __launch_bounds__(BLOCK) sssp_async_ell(SsspArgs a, const uint32
 // (gb_worklist.cuh) as single ids, at most once each (a queued flag per
 // region); a bucket ends when no region is queued and no CTA holds one.
 
-// 2048-vertex regions, two CTAs per SM: on the 4096^2 grid 27.4 ms against
-// 29.3 ms for 4096 (one per SM) and 28.7 ms for 1024 (four per SM)
+// 2048-vertex regions (27.4 ms on the 4096^2 grid against 29.3 for 4096 and
+// 28.7 for 1024, measured with two CTAs per SM), one CTA per SM: the CTAs
+// mostly wait for queued regions, and 96 registers a thread instead of 64
+// shorten a round (733 against 827 cycles per hop of a path; grid 16.9
+// against 17.4 ms)
 constexpr uint32_t kRegion = 2048;       // vertices per region (a multiple of 32)
 constexpr uint32_t kRegionArcs = 8192;   // arcs a region may hold in shared memory
 constexpr uint32_t kRegionOut = 128;     // outbox: relaxations of arcs leaving the region, per round
 constexpr uint32_t kRegionOutBufs = 8;   // outbox buffers (round k uses buffer k % 8)
 constexpr int kRegionBlock = 512;
-constexpr int kRegionPerSm = 2;
+constexpr int kRegionPerSm = 1;
 constexpr int kRegionRelax = 448;        // threads that relax (warps 0-13); warps 14 and 15 are the couriers
 static_assert(kRegion % kRegionBlock == 0, "a thread takes kRegion / kRegionBlock vertices of a region");
 
