@@ -944,7 +944,8 @@ constexpr uint32_t kRegionOutBufs = 8;   // outbox buffers (round k uses buffer 
 constexpr int kRegionBlock = 512;
 constexpr int kRegionPerSm = 1;
 constexpr int kRegionRelax = 448;        // threads that relax (warps 0-13); warps 14 and 15 are the couriers
-static_assert(kRegion % kRegionBlock == 0, "a thread takes kRegion / kRegionBlock vertices of a region");
+static_assert(kRegion % kRegionBlock == 0 && kRegion % 1024 == 0,
+              "a thread takes kRegion / kRegionBlock vertices, a lane kRegion / 1024 pending words");
 
 struct RegionArgs {
   uint32_t* pend;  // bitmap: vertex lowered from outside its region, to be expanded
@@ -1274,8 +1275,8 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
                 const bool ok = k + 1 < kRegionOutBufs || ld_acquire_cta(&s_odone) > nb;
                 s_obok[(k + 1) & 1] = ok ? 1u : 0u;
               }
-              s_bm[(k & 1) * (kRegion / 32) + lane] = 0u;
-              s_bm[(k & 1) * (kRegion / 32) + lane + 32] = 0u;
+#pragma unroll
+              for (uint32_t t = 0; t < kRegion / 1024; ++t) s_bm[(k & 1) * (kRegion / 32) + lane + 32 * t] = 0u;
               // the inbox flag is cleared before the bits are taken (the
               // courier sets bits, then the flag)
               uint32_t f = 0;
@@ -1360,14 +1361,16 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
             uint32_t qr = 0;
             if (lane == 0) qr = ld_acquire_cta(&s_qreq);
             qr = __shfl_sync(kFull, qr, 0);
-            uint32_t b0 = 0, b1 = 0;
-            if (lane < nw) {
-              b0 = *reinterpret_cast<volatile uint32_t*>(&ra.pend[pw0 + lane]);
-              if (b0) b0 = atomicExch(&ra.pend[pw0 + lane], 0u);
-            }
-            if (lane + 32 < nw) {
-              b1 = *reinterpret_cast<volatile uint32_t*>(&ra.pend[pw0 + lane + 32]);
-              if (b1) b1 = atomicExch(&ra.pend[pw0 + lane + 32], 0u);
+            // a lane takes pending words lane, lane + 32, ...
+            uint32_t bw[kRegion / 1024];
+#pragma unroll
+            for (uint32_t t = 0; t < kRegion / 1024; ++t) {
+              const uint32_t w = lane + 32 * t;
+              bw[t] = 0u;
+              if (w < nw) {
+                bw[t] = *reinterpret_cast<volatile uint32_t*>(&ra.pend[pw0 + w]);
+                if (bw[t]) bw[t] = atomicExch(&ra.pend[pw0 + w], 0u);
+              }
             }
             // no fence: the exchanges have returned, and a writer's atomicMin
             // had returned before it set the bit (region_touch)
@@ -1388,14 +1391,12 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
                 if (lane == 0) atomicOr(&s_inbm[w], mk);
               }
             };
-            for (unsigned m = __ballot_sync(kFull, b0 != 0u); m; m &= m - 1) {
-              const int src = __ffs(m) - 1;
-              take_word((uint32_t)src, __shfl_sync(kFull, b0, src));
-            }
-            for (unsigned m = __ballot_sync(kFull, b1 != 0u); m; m &= m - 1) {
-              const int src = __ffs(m) - 1;
-              take_word((uint32_t)src + 32, __shfl_sync(kFull, b1, src));
-            }
+#pragma unroll
+            for (uint32_t t = 0; t < kRegion / 1024; ++t)
+              for (unsigned m = __ballot_sync(kFull, bw[t] != 0u); m; m &= m - 1) {
+                const int src = __ffs(m) - 1;
+                take_word((uint32_t)src + 32 * t, __shfl_sync(kFull, bw[t], src));
+              }
             if (any && lane == 0) st_release_cta(&s_in_any, 1u);
             if (qr == q) break;
             if ((pass & 63u) == 0 && globaltimer_ns() > deadline) {
