@@ -1143,16 +1143,33 @@ def main() -> None:
             h = g["host"]
             pinned.append((pinned_copy(h.end_offs), pinned_copy(h.col),
                            pinned_copy(h.w_u32) if h.w_u32 is not None else None))
-        host_out = [pinned_copy(np.zeros(g["host"].n, npdt)) for g in job.graphs]
+        tdt = {np.dtype(np.uint32): torch.int32, np.dtype(np.float32): torch.float32}[np.dtype(npdt)]
+        host_out = [torch.empty(g["host"].n, dtype=tdt, pin_memory=True) for g in job.graphs]
+        dev_out = [torch.empty(g["host"].n, dtype=tdt, device=f"cuda:{dev}") for g in job.graphs]
         h2d = sum(a.nbytes + b.nbytes + (c.nbytes if c is not None else 0) for a, b, c in pinned)
-        d2h = sum(o.nbytes for o in host_out)
+        d2h = sum(o.numel() * o.element_size() for o in host_out)
         from galois_b200.graph import HostCSR
 
+        # The graphs are independent: the one whose kernel runs longest is
+        # uploaded and started first (asynchronously, into a device buffer),
+        # and the others are uploaded while it runs (gb_graph_upload copies
+        # host inputs on a stream of its own); one readback at the end.
+        order = sorted(range(len(job.graphs)), key=lambda gi: -float(stats[gi].get("kernel_ms", 0.0)))
+
         def e2e_step():
-            for gi, g in enumerate(job.graphs):
-                a, b, c = pinned[gi]
-                with DeviceGraph(HostCSR(a, b, c), symmetric=g["symmetric"], device=dev) as dg:
-                    job.device_call(dg, gi, host_out[gi])
+            live = []
+            try:
+                for gi in order:
+                    a, b, c = pinned[gi]
+                    dg = DeviceGraph(HostCSR(a, b, c), symmetric=job.graphs[gi]["symmetric"], device=dev)
+                    live.append(dg)
+                    job.device_call(dg, gi, dev_out[gi])
+                for gi in order:
+                    host_out[gi].copy_(dev_out[gi], non_blocking=True)
+                torch.cuda.current_stream(dev).synchronize()
+            finally:
+                for dg in live:
+                    dg.free()
 
         for _ in range(2):  # untimed: the first calls also fill the allocator cache and page in the buffers
             e2e_step()
@@ -1171,7 +1188,8 @@ def main() -> None:
                        # host varies from step to step, and value is over all of them
                        "step_ms": step_ms,
                        "path": "gb_graph_upload (pinned host CSR, file order: a one-shot call does not "
-                               "amortise gb_graph_reorder) + kernel + host output copy + gb_graph_free"}
+                               "amortise gb_graph_reorder) + kernel into a device buffer, the graphs' uploads "
+                               "overlapping the longest kernel + one host readback + gb_graph_free"}
     for dg in dgs:
         dg.free()
     # ---- the other plain kernels on their configurations (one GPU) ------------

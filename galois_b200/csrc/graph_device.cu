@@ -320,6 +320,22 @@ using namespace gb;
 
 extern "C" {
 
+// A non-blocking stream per device for uploads, kept for the process: an
+// upload's copies then overlap kernels that other streams run on the GPU
+// (copies on the legacy default stream would wait for them).  Falls back to
+// the default stream if one cannot be created.
+static cudaStream_t upload_stream(int device) {
+  static std::mutex mu;
+  static std::vector<cudaStream_t> streams;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)streams.size() <= device) streams.resize(device + 1, nullptr);
+  if (!streams[device] && cudaStreamCreateWithFlags(&streams[device], cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    streams[device] = nullptr;
+  }
+  return streams[device];
+}
+
 int gb_graph_upload(const uint64_t* end_offs, const uint32_t* col, const uint32_t* w_u32,
                     const float* w_f32, uint32_t n, uint64_t m, int symmetric, int device,
                     gb_graph** out) {
@@ -350,7 +366,11 @@ int gb_graph_upload(const uint64_t* end_offs, const uint32_t* col, const uint32_
   if (w_u32 && (e = dalloc(&g->w, sizeof(uint32_t) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc w"));
   if (w_f32 && (e = dalloc(&g->wf, sizeof(float) * std::max<uint64_t>(m, 1))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc wf"));
   if ((e = pool_malloc_host(&g->pinned, 8192)) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
-  cudaStream_t s = 0;
+  // host inputs are ready now; device inputs may still be written by work
+  // queued on other streams, which the default stream waits for
+  const bool dev_in = is_device_ptr(end_offs) || (m && is_device_ptr(col)) || (w_u32 && is_device_ptr(w_u32)) ||
+                      (w_f32 && is_device_ptr(w_f32));
+  cudaStream_t s = dev_in ? cudaStream_t(0) : upload_stream(device);
   if ((e = cudaMemsetAsync(g->offs, 0, sizeof(uint64_t), s)) != cudaSuccess) return fail(cuda_fail(e, "memset"));
   if ((e = cudaMemcpyAsync(g->offs + 1, end_offs, sizeof(uint64_t) * n, cudaMemcpyDefault, s)) != cudaSuccess) return fail(cuda_fail(e, "copy offs"));
   if (m && (e = cudaMemcpyAsync(g->col, col, sizeof(uint32_t) * m, cudaMemcpyDefault, s)) != cudaSuccess) return fail(cuda_fail(e, "copy col"));

@@ -140,7 +140,12 @@ typedef struct gb_graph gb_graph;
 /* Upload a CSR to `device`.  end_offs: LC layout (n entries).  Either weight
  * array may be NULL.  symmetric != 0 declares in-edges == out-edges (the
  * -symmetricGraph flag, BoilerPlate.cpp:38-41), which enables pull/bottom-up
- * steps without a transpose.  Inputs may be host or device pointers. */
+ * steps without a transpose.  Inputs may be host or device pointers.
+ * Host inputs are copied on a stream of the library's own that does not wait
+ * for kernels running on other streams (an upload can overlap a kernel of
+ * another graph); device inputs are copied on the default stream, after the
+ * work queued before the call.  The call returns when the graph is on the
+ * device. */
 int gb_graph_upload(const uint64_t* end_offs, const uint32_t* col,
                     const uint32_t* w_u32, const float* w_f32, uint32_t n,
                     uint64_t m, int symmetric, int device, gb_graph** out);
