@@ -47,7 +47,8 @@ struct CcArgs {
   const uint64_t* __restrict__ offs;
   const uint32_t* __restrict__ col;
   uint32_t n;
-  int half;  // process only u > v (symmetric graph)
+  int half;    // process only u < v (symmetric graph)
+  int sorted;  // rows sorted ascending (relabelled graphs): a row's u < v arcs are its prefix
   uint32_t* p;
   SweepSched sched;
   CcCtl* ctl;
@@ -96,33 +97,25 @@ __device__ __forceinline__ void compress_all(CcArgs& a, uint64_t gtid, uint64_t 
   }
 }
 
-// Most frequent label among 1024 evenly spaced vertices (Afforest's estimate
+// Most frequent label among BLOCK evenly spaced vertices (Afforest's estimate
 // of the giant component), written to ctl->giant.  Called by every thread of
-// one CTA.
+// one CTA, one sample each (1024 samples with 1024 comparisons per sample
+// kept the other CTAs waiting 75 us on RMAT-24; any label is correct, the
+// estimate only decides which rows the next round may skip).
 template <int BLOCK>
 __device__ void sample_giant(const CcArgs& a, CcCtl* ctl) {
-  __shared__ uint32_t s_root[1024];
-  __shared__ uint32_t s_cnt[1024];
-  for (uint32_t i = threadIdx.x; i < 1024; i += BLOCK) {
-    const uint32_t v = (uint32_t)(((uint64_t)i * a.n) >> 10);
-    s_root[i] = a.p[v];
-  }
+  __shared__ uint32_t s_root[BLOCK];
+  __shared__ uint32_t s_best[2];
+  const uint32_t i = threadIdx.x;
+  s_root[i] = a.p[(uint32_t)(((uint64_t)i * a.n) / BLOCK)];
+  if (i == 0) s_best[0] = s_best[1] = 0;
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < 1024; i += BLOCK) {
-    uint32_t c = 0;
-    for (uint32_t j = 0; j < 1024; ++j) c += s_root[j] == s_root[i];
-    s_cnt[i] = c;
-  }
+  uint32_t c = 0;
+  for (uint32_t j = 0; j < BLOCK; ++j) c += s_root[j] == s_root[i];
+  // the count in the high bits, the sample's index in the low: one atomicMax
+  atomicMax(&s_best[0], (c << 16) | (BLOCK - 1 - i));
   __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t best = s_root[0], bestc = 0;
-    for (uint32_t i = 0; i < 1024; ++i)
-      if (s_cnt[i] > bestc) {
-        bestc = s_cnt[i];
-        best = s_root[i];
-      }
-    ctl->giant = best;
-  }
+  if (i == 0) ctl->giant = s_root[BLOCK - 1 - (s_best[0] & 0xFFFFu)];
 }
 
 template <int BLOCK>
@@ -148,20 +141,43 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
       break;
     }
     const bool skip_giant = a.half && r >= 1;
-    const bool all_dirs = !a.half || skip_giant;  // arcs u < v too
+    // the first sweep of a symmetric graph takes each edge once, as its arc
+    // u < v: on a degree-ordered graph that is a prefix of a hub's row (its
+    // neighbours of higher degree), and the gathered labels are the hubs'
+    const bool all_dirs = !a.half || skip_giant;  // arcs u > v too
     uint32_t* changed = &ctl->changed[r % 3];
     if (gtid == 0) ctl->changed[(r + 1) % 3] = 0;
     bool my_change = false;
     // Hook labels pv (of v, read once per vertex; a stale value is still a
     // label of v's component, so the union stays valid) and pu: the larger
     // goes under the smaller, checked before the atomic.
+    // When hi already hangs under another label c (p[hi] = c, read first,
+    // or returned by the atomic), the arc also joins c and lo, so the hook
+    // goes on with that pair: a label read once per row may be stale, and
+    // without this a vertex between two hubs would leave their trees apart
+    // for another round.  The larger of the pair falls every step (p[x] <= x);
+    // a pair still apart after 4 steps marks the round changed, and the next
+    // round scans a row of it (its two labels differ after the compression,
+    // so at most one is the giant one).
     auto hook = [&](bool valid, uint32_t pv, uint32_t pu) {
-      if (valid && pv != pu) {
-        const uint32_t hi = max(pv, pu), lo = min(pv, pu);
-        if (lo < a.p[hi]) {
-          atomicMin(&a.p[hi], lo);
+      if (!valid) return;
+      uint32_t x = pv, y = pu;
+      for (int step = 0; x != y; ++step) {
+        if (step == 4) {
           my_change = true;
+          return;
         }
+        const uint32_t hi = max(x, y), lo = min(x, y);
+        const uint32_t c = a.p[hi];
+        if (c == lo) return;
+        if (c < lo) {
+          x = c, y = lo;  // hi is under c already: join c and lo
+          continue;
+        }
+        const uint32_t old = atomicMin(&a.p[hi], lo);
+        if (old > lo) my_change = true;
+        if (old == hi || old == lo) return;  // hi was a root, or is under lo already
+        x = old, y = lo;                     // hi hung under old: join old and lo
       }
     };
     // Tasks as in sweep.cuh: 32-vertex chunks, then heavy-vertex tiles.  In
@@ -171,17 +187,20 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
     const uint64_t total = nchunks + a.sched.ntiles;
     // one tile of a heavy row: 8 column loads, then 8 label loads, per lane
     auto tile_fn = [&](uint32_t v, uint64_t b, uint64_t e) {
+      // a sorted row's u < v arcs end before the first u >= v
+      if (!all_dirs && a.sorted && ldg(a.col + b) >= v) return;  // warp-uniform
       const uint32_t pv = a.p[v];
       if (skip_giant && pv == giant) return;  // warp-uniform
       if (lane == 0) my_scanned += e - b;
       constexpr int UT = 8;
       for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
+        if (i0 > b && !all_dirs && a.sorted && ldg(a.col + i0) >= v) break;  // warp-uniform
         uint32_t u[UT], pu[UT];
 #pragma unroll
         for (int k = 0; k < UT; ++k) {
           const uint64_t i = i0 + lane + 32 * k;
           const uint32_t x = i < e ? ldg(a.col + i) : 0u;
-          u[k] = (i < e && (all_dirs || x > v)) ? x : 0xFFFFFFFFu;
+          u[k] = (i < e && (all_dirs || x < v)) ? x : 0xFFFFFFFFu;
         }
 #pragma unroll
         for (int k = 0; k < UT; ++k) pu[k] = u[k] != 0xFFFFFFFFu ? a.p[u[k]] : 0u;
@@ -206,7 +225,7 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
             b, d, (uint32_t)v64,
             [&](bool valid, uint64_t e, uint32_t v) {
               const uint32_t u = valid ? ldg(a.col + e) : 0u;
-              return (valid && (all_dirs || u > v)) ? u : 0xFFFFFFFFu;
+              return (valid && (all_dirs || u < v)) ? u : 0xFFFFFFFFu;
             },
             [&](bool, uint64_t, uint32_t u, uint32_t) { return u != 0xFFFFFFFFu ? a.p[u] : 0u; },
             [&](bool, uint32_t owner, uint32_t, uint32_t u, uint32_t pu) {
@@ -224,10 +243,11 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
     if (__any_sync(kFull, my_change) && lane == 0 && *reinterpret_cast<volatile uint32_t*>(changed) == 0)
       atomicOr(changed, 1u);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
+    if (gtid == 0) ctl->rounds = r + 1;
+    // a round that hooked nothing leaves every label a root already
+    if (*reinterpret_cast<volatile uint32_t*>(changed) == 0) break;
     compress_all(a, gtid, gthreads);
     if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
-    if (gtid == 0) ctl->rounds = r + 1;
-    if (*reinterpret_cast<volatile uint32_t*>(changed) == 0) break;
     if (r == 0 && a.half) {
       if (blockIdx.x == 0) sample_giant<BLOCK>(a, ctl);
       if (!grid_barrier(&ctl->bar, gridDim.x, &ctl->err, deadline)) return;
@@ -319,6 +339,7 @@ int run_cc(gb_graph* g, int algo, uint32_t* label_out, gb_stats* stats, cudaStre
   a.col = g->col;
   a.n = n;
   a.half = g->symmetric ? 1 : 0;
+  a.sorted = (g->perm && g->order != GB_ORDER_DEGREE_UNSORTED && g->m < (1ull << 31)) ? 1 : 0;
   a.sched = sched;
   a.max_rounds = 1u << 20;
   GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(CcCtl), s));
