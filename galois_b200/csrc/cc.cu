@@ -191,10 +191,10 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
       if (!all_dirs && a.sorted && ldg(a.col + b) >= v) return;  // warp-uniform
       const uint32_t pv = a.p[v];
       if (skip_giant && pv == giant) return;  // warp-uniform
-      if (lane == 0) my_scanned += e - b;
       constexpr int UT = 8;
       for (uint64_t i0 = b; i0 < e; i0 += 32 * UT) {
         if (i0 > b && !all_dirs && a.sorted && ldg(a.col + i0) >= v) break;  // warp-uniform
+        if (lane == 0) my_scanned += e - i0 < 32 * UT ? e - i0 : (uint64_t)(32 * UT);  // the arcs read
         uint32_t u[UT], pu[UT];
 #pragma unroll
         for (int k = 0; k < UT; ++k) {
