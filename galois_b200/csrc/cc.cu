@@ -49,6 +49,7 @@ struct CcArgs {
   uint32_t n;
   int half;    // process only u < v (symmetric graph)
   int sorted;  // rows sorted ascending (relabelled graphs): a row's u < v arcs are its prefix
+  uint32_t vend;  // rows from vend on are empty (degree-ordered graphs; else n)
   uint32_t* p;
   SweepSched sched;
   CcCtl* ctl;
@@ -90,7 +91,9 @@ __device__ __forceinline__ void link(uint32_t* p, uint32_t a, uint32_t b) {
 }
 
 __device__ __forceinline__ void compress_all(CcArgs& a, uint64_t gtid, uint64_t gthreads) {
-  for (uint64_t v = gtid; v < a.n; v += gthreads) {
+  // on a symmetric graph a vertex without arcs keeps its own label
+  const uint32_t vn = a.half ? a.vend : a.n;
+  for (uint64_t v = gtid; v < vn; v += gthreads) {
     uint32_t x = a.p[v];
     while (x != a.p[x]) x = a.p[x];
     a.p[v] = x;
@@ -107,7 +110,7 @@ __device__ void sample_giant(const CcArgs& a, CcCtl* ctl) {
   __shared__ uint32_t s_root[BLOCK];
   __shared__ uint32_t s_best[2];
   const uint32_t i = threadIdx.x;
-  s_root[i] = a.p[(uint32_t)(((uint64_t)i * a.n) / BLOCK)];
+  s_root[i] = a.p[(uint32_t)(((uint64_t)i * a.vend) / BLOCK)];  // vertices with arcs
   if (i == 0) s_best[0] = s_best[1] = 0;
   __syncthreads();
   uint32_t c = 0;
@@ -183,7 +186,7 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
     // Tasks as in sweep.cuh: 32-vertex chunks, then heavy-vertex tiles.  In
     // a chunk each lane reads its vertex's label once; the expansion (4 steps
     // of column and label loads in flight) takes the owner's label by shuffle.
-    const uint64_t nchunks = ((uint64_t)a.n + 31) >> 5;
+    const uint64_t nchunks = ((uint64_t)a.vend + 31) >> 5;  // rows from vend on are empty
     const uint64_t total = nchunks + a.sched.ntiles;
     // one tile of a heavy row: 8 column loads, then 8 label loads, per lane
     auto tile_fn = [&](uint32_t v, uint64_t b, uint64_t e) {
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
         const uint64_t v64 = (t << 5) + lane;
         uint64_t b = 0;
         uint32_t d = 0, pv = 0;
-        if (v64 < a.n) {
+        if (v64 < a.vend) {
           b = ldg(a.offs + v64);
           const uint64_t dd = ldg(a.offs + v64 + 1) - b;
           d = dd > a.sched.heavy ? 0u : (uint32_t)dd;
@@ -340,6 +343,7 @@ int run_cc(gb_graph* g, int algo, uint32_t* label_out, gb_stats* stats, cudaStre
   a.n = n;
   a.half = g->symmetric ? 1 : 0;
   a.sorted = (g->perm && g->order != GB_ORDER_DEGREE_UNSORTED && g->m < (1ull << 31)) ? 1 : 0;
+  a.vend = g->perm ? std::max<uint32_t>(g->zero_from, 1u) : n;
   a.sched = sched;
   a.max_rounds = 1u << 20;
   GB_CUDA(cudaMemsetAsync(a.ctl, 0, sizeof(CcCtl), s));
