@@ -50,6 +50,7 @@ struct BfsArgs {
   const uint64_t* __restrict__ in_offs;  // nullptr: push only
   const uint32_t* __restrict__ in_col;
   uint32_t n;
+  uint32_t pull_end;  // bottom-up steps scan vertices below it (vertices from it on have no in-arcs)
   uint64_t m;
   uint32_t src;
   uint32_t* level;
@@ -241,12 +242,12 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(BfsArgs a) {
       // word of `visited` and of the next frontier in a pull level, so both
       // are written with plain stores of the warp's ballot.  The next
       // frontier is left as a bitmap (no queue).
-      for (uint64_t base = gtid - lane; base < a.n; base += gthreads) {
+      for (uint64_t base = gtid - lane; base < a.pull_end; base += gthreads) {
         const uint64_t u64 = base + lane;
         bool found = false;
         const uint32_t u = (uint32_t)u64;
         const uint32_t vword = base < a.n ? a.visited[base >> 5] : ~0u;
-        if (u64 < a.n && !(vword & (1u << lane))) {
+        if (u64 < a.pull_end && !(vword & (1u << lane))) {
           const uint64_t b = ldg(a.in_offs + u), e = ldg(a.in_offs + u + 1);
           uint64_t i = b;
           for (; i < e; ++i) {
@@ -330,6 +331,9 @@ int run_bfs(gb_graph* g, uint32_t src, uint32_t* level_out, gb_stats* stats, cud
     a.in_col = g->t_col;
   }
   a.n = n;
+  // a symmetric graph's in-arcs are its arcs: on a degree-ordered one the
+  // vertices from zero_from on have none, and no bottom-up step finds them
+  a.pull_end = g->symmetric && g->perm ? g->zero_from : n;
   a.m = g->m;
   a.src = src;
   a.heavy = t.heavy_degree;
@@ -429,6 +433,7 @@ int run_bfs_sources(gb_graph* g, const uint32_t* d_srcs, uint32_t k, uint32_t* d
     a.in_col = g->col;
   }
   a.n = n;
+  a.pull_end = g->symmetric && g->perm ? g->zero_from : n;
   a.m = g->m;
   a.src = 0xFFFFFFFFu;
   a.heavy = t.heavy_degree;
@@ -599,6 +604,7 @@ extern "C" int gb_bfs_noalloc(const uint64_t* offs, const uint32_t* col, uint32_
     a.in_col = col;
   }
   a.n = n;
+  a.pull_end = n;
   a.m = m;
   a.src = src;
   a.heavy = kNoAllocHeavy;
