@@ -944,8 +944,8 @@ constexpr uint32_t kRegionOutBufs = 8;   // outbox buffers (round k uses buffer 
 constexpr int kRegionBlock = 512;
 constexpr int kRegionPerSm = 1;
 constexpr int kRegionRelax = 448;        // threads that relax (warps 0-13); warps 14 and 15 are the couriers
-static_assert(kRegion % kRegionBlock == 0 && kRegion % 1024 == 0,
-              "a thread takes kRegion / kRegionBlock vertices, a lane kRegion / 1024 pending words");
+static_assert(kRegion % 1024 == 0, "a lane takes kRegion / 1024 pending words");
+constexpr int kRegionPer = (kRegion + kRegionBlock - 1) / kRegionBlock;  // vertices of a region per thread
 
 struct RegionArgs {
   uint32_t* pend;  // bitmap: vertex lowered from outside its region, to be expanded
@@ -1117,7 +1117,7 @@ __device__ __forceinline__ void region_load_rows(const SsspArgs& a, uint32_t bas
   for (uint32_t i = (nv & ~3u) + tid; i < nv; i += kRegionBlock) s_dist[i] = __ldcg(a.dist + base + i);
   // a thread's vertices all at once: their offsets, then their arcs (two
   // dependent loads in all, not two per vertex)
-  constexpr int kPer = kRegion / kRegionBlock;
+  constexpr int kPer = kRegionPer;
   uint64_t b[kPer], e[kPer];
 #pragma unroll
   for (int t = 0; t < kPer; ++t) {
@@ -1463,7 +1463,7 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
       // write the lowered distances back (a thread's global distances read
       // at once); those beyond the bucket join the far pile
       {
-        constexpr int kPer = kRegion / kRegionBlock;
+        constexpr int kPer = kRegionPer;
         uint32_t gd[kPer];
 #pragma unroll
         for (int t = 0; t < kPer; ++t) {
