@@ -96,3 +96,61 @@ def test_pool_reuses_blocks_and_trims(cuda_device):
     _lib.check(_lib.lib.gb_pool_trim(), "gb_pool_trim")
     with DeviceGraph(g, symmetric=True) as dg:  # a fresh allocation after the trim
         assert (dg.bfs(int(perm[0])) == want).all()
+
+
+def test_upload_overlaps_another_graphs_kernel(cuda_device):
+    """gb_graph_upload copies host arrays on a stream of the library's own, so
+    a graph can be uploaded while another graph's kernel runs asynchronously
+    into a device buffer; both results stay exact."""
+    import torch
+
+    from galois_b200 import grid2d
+
+    ga = grid2d(512, 512)
+    assign_weights_u32(ga, 1, 255, seed=5)
+    want_a = oracle.sssp_dijkstra(ga, 0)
+    gb, perm = rmat(14, 8, seed=6, symmetrize=True)
+    src = int(perm[0])
+    want_b = oracle.bfs_serial(gb, src)
+    with DeviceGraph(ga, symmetric=True) as da:
+        out_a = torch.empty(ga.n, dtype=torch.int32, device="cuda")
+        da.sssp(0, 13, out=out_a)  # queued on torch's stream, not waited for
+        with DeviceGraph(gb, symmetric=True) as db:  # uploaded meanwhile
+            lev_b = db.bfs(src)
+        torch.cuda.current_stream().synchronize()
+        assert (out_a.cpu().numpy().view(np.uint32) == want_a).all()
+        assert (lev_b == want_b).all()
+
+
+def test_upload_from_device_arrays_waits_for_queued_writes(cuda_device):
+    """Device inputs are copied on the default stream, after the work queued
+    before the call: arrays whose writes are still queued behind a long
+    kernel on torch's stream upload complete."""
+    import ctypes as C
+
+    import torch
+
+    from galois_b200 import _lib
+
+    g, perm = rmat(14, 8, seed=7, symmetrize=True)
+    src = int(perm[0])
+    want = oracle.bfs_serial(g, src)
+    end_h = torch.from_numpy(g.end_offs.astype(np.int64)).pin_memory()
+    col_h = torch.from_numpy(g.col.view(np.int32).copy()).pin_memory()
+    end_d = torch.zeros(g.n, dtype=torch.int64, device="cuda")
+    col_d = torch.zeros(g.m, dtype=torch.int32, device="cuda")
+    x = torch.randn(2048, 2048, device="cuda")
+    for _ in range(8):  # keep torch's stream busy before the writes
+        x = torch.tanh(x @ x)
+    end_d.copy_(end_h, non_blocking=True)
+    col_d.copy_(col_h, non_blocking=True)
+    handle = C.c_void_p()
+    _lib.check(_lib.lib.gb_graph_upload(C.c_void_p(end_d.data_ptr()), C.c_void_p(col_d.data_ptr()), None, None,
+                                        g.n, g.m, 1, 0, C.byref(handle)), "gb_graph_upload")
+    try:
+        lev = np.empty(g.n, np.uint32)
+        _lib.check(_lib.lib.gb_bfs(handle, src, C.c_void_p(lev.ctypes.data), None, None), "gb_bfs")
+        assert (lev == want).all()
+    finally:
+        _lib.lib.gb_graph_free(handle)
+    assert torch.isfinite(x).all()
