@@ -216,12 +216,18 @@ __global__ void __launch_bounds__(BLOCK) cc_labelprop(CcArgs a) {
         const uint64_t v64 = (t << 5) + lane;
         uint64_t b = 0;
         uint32_t d = 0, pv = 0;
+        bool mine = false;
         if (v64 < a.vend) {
+          pv = a.p[v64];
+          mine = !(skip_giant && pv == giant);
+        }
+        // a later round reads a chunk's labels first: most chunks lie inside
+        // the giant label and need no offsets
+        if (skip_giant && !__any_sync(kFull, mine)) continue;  // warp-uniform
+        if (mine) {
           b = ldg(a.offs + v64);
           const uint64_t dd = ldg(a.offs + v64 + 1) - b;
           d = dd > a.sched.heavy ? 0u : (uint32_t)dd;
-          pv = a.p[v64];
-          if (skip_giant && pv == giant) d = 0;
         }
         my_scanned += d;
         warp_expand_mlp<4, uint32_t>(
