@@ -922,8 +922,8 @@ __global__ void __launch_bounds__(BLOCK) sssp_async_ell(SsspArgs a, const uint32
 // region r and most arcs stay inside their region.  A CTA takes one queued
 // region at a time, loads its distances, row offsets and arcs into shared
 // memory and relaxes to a local fixed point inside the current bucket: a hop
-// inside the region is a shared-memory atomic and a CTA barrier, not a global
-// round trip.  An arc that leaves the region lowers the global distance and
+// inside the region is a shared-memory atomic and a barrier of the relaxing
+// warps, not a global round trip.  An arc that leaves the region lowers the global distance and
 // then either marks the target pending (one bit per vertex) and queues the
 // target's region, or files the target in the far pile.  Global distances
 // stay authoritative: the region writes its lowered distances back with
@@ -1248,9 +1248,10 @@ __global__ void __launch_bounds__(kRegionBlock, kRegionPerSm) sssp_region(SsspAr
       // the last round (a release), warp 13 clears the bitmap, moves the
       // inbox into the next round's list and decides whether the next round
       // may use its buffer (an acquire), so the fences (about 400 cycles
-      // each) stay off the other warps' path.  When a round lists nothing, the relaxers
-      // ask the couriers to finish (the outbox drained, one more poll) and all
-      // 512 threads meet; the visit goes on if the inbox holds vertices.
+      // each) stay off the other warps' path.  When a round lists nothing,
+      // the relaxers ask the couriers to finish (the outbox drained, one more
+      // poll) and all 512 threads meet; the visit goes on if the inbox holds
+      // vertices.
       constexpr uint32_t kBooks = kRegionRelax / 32 - 1;  // the book-keeping warp
       uint32_t k = 0, jo = 0;
       for (uint32_t q = 1;; ++q) {
