@@ -115,6 +115,7 @@ __global__ void gather_out_kernel(const T* __restrict__ res, const uint32_t* __r
 // component sends most threads to one word: read it first (from L2) and only
 // issue the atomic when it would lower the value, so after the first few
 // updates the threads only read.
+// over internal ids [0, n): the least original id under each label
 __global__ void label_min_kernel(const uint32_t* __restrict__ lab, const uint32_t* __restrict__ perm, uint32_t n,
                                  uint32_t* __restrict__ minorig) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -124,12 +125,16 @@ __global__ void label_min_kernel(const uint32_t* __restrict__ lab, const uint32_
   }
 }
 
-// out[original v] = minorig[lab[iperm[v]]]
+// out[original v] = minorig[lab[iperm[v]]]; a vertex from `single` on (no
+// arcs on a symmetric graph: a component of its own) is its own answer
 __global__ void label_out_kernel(const uint32_t* __restrict__ lab, const uint32_t* __restrict__ minorig,
-                                 const uint32_t* __restrict__ iperm, uint32_t n, uint32_t* __restrict__ out) {
+                                 const uint32_t* __restrict__ iperm, uint32_t n, uint32_t single,
+                                 uint32_t* __restrict__ out) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += stride)
-    out[v] = minorig[lab[iperm[v]]];
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += stride) {
+    const uint32_t iv = iperm[v];
+    out[v] = iv >= single ? (uint32_t)v : minorig[lab[iv]];
+  }
 }
 
 // Largest reached level, ties to the smallest id: key = level << 32 | ~v.
@@ -266,12 +271,16 @@ int finish_f32(gb_graph* g, const float* res, float* out, cudaStream_t s) {
 
 int finish_labels(gb_graph* g, const uint32_t* res, uint32_t* out, cudaStream_t s) {
   const uint32_t n = g->n;
+  // on a symmetric degree-ordered graph the vertices from zero_from on have
+  // no arcs: components of their own, labelled by themselves, which no other
+  // label reaches (a component's least id is below zero_from)
+  const uint32_t single = g->symmetric ? g->zero_from : n;
   uint32_t* minorig = result_buf(g, 1);
-  GB_CUDA(cudaMemsetAsync(minorig, 0xFF, sizeof(uint32_t) * n, s));
-  label_min_kernel<<<blocks_for(g, n), 256, 0, s>>>(res, g->perm, n, minorig);
+  GB_CUDA(cudaMemsetAsync(minorig, 0xFF, sizeof(uint32_t) * single, s));
+  if (single) label_min_kernel<<<blocks_for(g, single), 256, 0, s>>>(res, g->perm, single, minorig);
   const bool dev = is_device_ptr(out);
   uint32_t* dst = dev ? out : result_buf(g, 2);
-  label_out_kernel<<<blocks_for(g, n), 256, 0, s>>>(res, minorig, g->iperm, n, dst);
+  label_out_kernel<<<blocks_for(g, n), 256, 0, s>>>(res, minorig, g->iperm, n, single, dst);
   GB_CUDA(cudaGetLastError());
   return dev ? GB_OK : copy_out(out, dst, sizeof(uint32_t) * n, s);
 }
